@@ -1,0 +1,358 @@
+"""Benchmark of the BSE build+solve hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Workload (one step = one system): the seeded synthetic 22-orbital 3-atom
+hexagonal model, k mesh 60 x 60 (BSE dimension 14400), 2 valence + 2
+conduction bands, real-space Keldysh interaction r0 = 40 A, eps_m = 1,
+eps_s = 4.5, direct term only.  The engine arm runs the mixed-precision path:
+device band solve, interaction tables, assembly of the split-BF16 kernel with
+the FP64 band diagonal, and the block Davidson for the lowest 8 states.
+
+value:  seconds per system with the model already resident on the device
+        (max over ranks of the device time / systems processed by all ranks).
+e2e:    same through the public C ABI from host buffers: upload of the model
+        and k mesh, build, solve, download of energies and eigenvectors.
+The reference arm times the CPU restatement of the reference (the oracle; the
+reference itself needs Armadillo/LAPACK/ARPACK, absent on this image) on the
+host cores, on bounded samples extrapolated to the full system.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BSE build+solve s/system & TC util, mixed vs FP64 on GPU at ≤1e-4 eV error"
+WORKLOAD = dict(model="synthetic hexagonal 8+7+7 orbitals (seed 1234)", ncell=60, nv=2, nc=2, nstates=8,
+                params=[1.0, 4.5, 40.0], mode="realspace", exchange=False)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--ncell", type=int, default=WORKLOAD["ncell"])
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return p.parse_args()
+
+
+def dist_init(n):
+    import torch
+    import torch.distributed as dist
+    if n > 1 or "RANK" in os.environ:
+        if not dist.is_initialized():
+            import datetime
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        return dist.get_rank(), dist.get_world_size(), int(os.environ.get("LOCAL_RANK", 0))
+    return 0, 1, 0
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile(prefix="clk", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+# ------------------------------------------------------------------ reference / CPU arm
+def cpu_sample(ncell: int, budget_s: float = 12.0):
+    """Time the CPU restatement (oracle) on bounded samples of the workload and
+    extrapolate to one full system.  Returns (seconds/system, description, threads)."""
+    from oracle.oracle import OracleExciton, OracleSystem
+    from xatu_b200.synthetic import synthetic_hexagonal
+    si = synthetic_hexagonal(seed=1234).systemInfo
+    s = OracleSystem(si.ndim, si.bravaisLattice, si.motif, si.norbitals, si.bravaisVectors, si.hamiltonian,
+                     int(si.filling))
+    ex = OracleExciton(s, ncell, 2, 0, WORKLOAD["params"])
+    ex.brillouin_zone_mesh(ncell)
+    t0 = time.perf_counter()
+    ex.initialize_hamiltonian()          # band solve (numpy LAPACK) + motif FT (C, OpenMP), full size
+    t_init = time.perf_counter() - t0
+    N = ex.N
+    # assembly: rows [0, r) of the upper triangle, scaled by the element count
+    r = max(1, min(N, int(N * 0.05)))
+    t0 = time.perf_counter()
+    ex.bs_rows(0, r)
+    t_rows = time.perf_counter() - t0
+    elems = sum(N - i for i in range(r))
+    t_build = t_rows * (N * (N + 1) / 2) / elems
+    # dense solve: LAPACK zheevd at a smaller N' scaled by (N / N')^3
+    n2 = 3072
+    rng = np.random.default_rng(0)
+    A = rng.normal(size=(n2, n2)) + 1j * rng.normal(size=(n2, n2))
+    A = A + A.conj().T
+    t0 = time.perf_counter()
+    np.linalg.eigh(A)
+    t_small = time.perf_counter() - t0
+    t_solve = t_small * (N / n2) ** 3
+    threads = os.cpu_count() or 1
+    desc = (f"oracle (C/OpenMP + numpy LAPACK) on {threads} host threads: full band solve + motif FT "
+            f"({t_init:.2f} s), {r} of {N} BSE rows ({t_rows:.2f} s) scaled to the full triangle, "
+            f"zheevd at N={n2} ({t_small:.2f} s) scaled by (N/{n2})^3")
+    return t_init + t_build + t_solve, desc, threads
+
+
+def run_reference(args):
+    rank, world, _ = dist_init(args.gpus)
+    if rank != 0:
+        return
+    W, K = args.warmup, args.steps
+    vals = []
+    desc, threads = "", 1
+    for i in range(W + K):
+        v, desc, threads = cpu_sample(args.ncell)
+        if i >= W:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s/system", "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD['model']}, Nk={args.ncell}x{args.ncell}, 2v+2c, N={args.ncell**2*4}",
+                       "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": "s/system", "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": "s/system", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ engine arm
+def run_engine(args):
+    import torch
+    rank, world, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    from xatu_b200 import _lib as L
+    from xatu_b200.exciton import ExcitonTB
+    from xatu_b200.synthetic import synthetic_hexagonal
+
+    ncell, nst = args.ncell, WORKLOAD["nstates"]
+    cfg = synthetic_hexagonal(seed=1234 + rank)      # independent system per rank (weak scaling)
+    ex = ExcitonTB(cfg, ncell, 2, 0, WORKLOAD["params"], device=local)
+    ex.brillouinZoneMesh(ncell)
+    stream = torch.cuda.Stream()
+    L.check(L.lib().xatu_ctx_set_stream(ex.ctx, ctypes.c_void_p(stream.cuda_stream)), ex.ctx)
+    lib = L.lib()
+    N = ex.excitonbasisdim
+    ev = np.zeros(nst)
+
+    def step_resident():
+        ex._call("xatu_bands_compute")
+        ex._call("xatu_interaction_build")
+        ex._call("xatu_bse_build", L.PREC_MIXED)
+        ex._call("xatu_bse_solve", L.SOLVER_DAVIDSON, nst, L.ptr(ev), None)
+
+    # host inputs for e2e (pinned)
+    s = ex.system
+    ham_shape = s.hamiltonianMatrices.shape
+    host = {"ham": torch.from_numpy(s.hamiltonianMatrices.view(np.float64)).pin_memory(),
+            "kp": torch.from_numpy(s.kpoints.copy()).pin_memory()}
+    eigvec = torch.empty((nst, N, 2), dtype=torch.float64).pin_memory()
+    eigval = np.zeros(nst)
+
+    def step_e2e():
+        ex.system.hamiltonianMatrices = host["ham"].numpy().view(np.complex128).reshape(ham_shape)
+        ex.system.kpoints = host["kp"].numpy()
+        ex.initializeHamiltonian()          # uploads system + k mesh, band solve, tables
+        ex._call("xatu_bse_build", L.PREC_MIXED)
+        ex._call("xatu_bse_solve", L.SOLVER_DAVIDSON, nst, L.ptr(eigval), ctypes.c_void_p(eigvec.data_ptr()))
+
+    ex.initializeHamiltonian()
+    for _ in range(args.warmup):
+        step_resident()
+    torch.cuda.synchronize()
+    launches0 = ex.kernelLaunches()
+    clk = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    asm_ms, solve_ms, iters, hx_ms, hx_n = [], [], [], [], []
+    hx_path = -1
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_resident()
+        st = ex.stageTimes()
+        asm_ms.append(st["assembly"])
+        solve_ms.append(st["solve"])
+        iters.append(ex.davidsonStats()[0])
+        n_hx, ms_hx, hx_path = ex.kernelStats("hx")
+        hx_ms.append(ms_hx)
+        hx_n.append(n_hx)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.stop()
+    gpu_launches = ex.kernelLaunches() - launches0
+    t_step = e0.elapsed_time(e1) / 1e3 / args.steps
+    t_step = dist_max(t_step, world)
+    value = t_step / world
+
+    # e2e through the public API from host buffers
+    for _ in range(1):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier(world)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    f0.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - w0) / args.steps
+    t_e2e = max(f0.elapsed_time(f1) / 1e3 / args.steps, wall)
+    t_e2e = dist_max(t_e2e, world) / world
+    h2d = s.hamiltonianMatrices.nbytes + s.kpoints.nbytes + s.meshBZ.nbytes + s.motif.nbytes + \
+        s.unitCellList.nbytes + s.bravaisLattice.nbytes
+    d2h = eigval.nbytes + eigvec.numel() * 8
+
+    # rooflines (HBM-bound kernels; algorithmic bytes per launch / CUDA-event launch time):
+    #  * assembly: writes K (two BF16 planes, 8 B per complex element) + the FP64 diagonal;
+    #  * K.X product: reads K (8 B per element), the BF16 operand planes (2 x 2b x 2N x 2 B)
+    #    and adds into Y (N x 2b FP32).
+    hbm, bf16, src = peaks()
+    asm_s = statistics.median(asm_ms) / 1e3
+    asm_bytes = N * N * 8 + N * 8
+    kernels = [{"kernel": "bse_assemble_tile_kernel<float,2,2,3,mixed>", "bound": "hbm",
+                "achieved": asm_bytes / asm_s / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": asm_bytes / asm_s / 1e9 / hbm, "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_launch": asm_bytes, "launch_ms": asm_s * 1e3, "launches_per_step": 1}]
+    calls = sum(hx_n)
+    if calls:
+        hx_s = sum(hx_ms) / calls / 1e3
+        ng = 32 if nst <= 8 else 64
+        hx_bytes = N * N * 8 + 2 * ng * 2 * N * 2 + N * ng * 4
+        kernels.append({"kernel": "hx_tcgen05_kernel" if hx_path == 2 else "hx_cuda_core_kernel", "bound": "hbm",
+                        "achieved": hx_bytes / hx_s / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": hx_bytes / hx_s / 1e9 / hbm, "peak_source": src, "traffic": None,
+                        "algorithmic_bytes_per_launch": hx_bytes, "launch_ms": hx_s * 1e3,
+                        "launches_per_step": calls / len(hx_n)})
+    roofline = max(kernels, key=lambda k: k["launch_ms"] * k["launches_per_step"])
+
+    extra = {"davidson_iterations": statistics.median(iters), "roofline_kernels": kernels,
+             "stage_ms": {"assembly": statistics.median(asm_ms), "solve": statistics.median(solve_ms)}}
+    # FP64 plain path on the same system (outside the timed region): FP64 build + dense FP64 solve
+    if not args.no_fp64 and rank == 0:
+        w_mixed = ev.copy()
+        ex._call("xatu_bse_build", L.PREC_FP64)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        allv = np.zeros(N)
+        t0.record(stream)
+        ex._call("xatu_bands_compute")
+        ex._call("xatu_interaction_build")
+        ex._call("xatu_bse_build", L.PREC_FP64)
+        ex._call("xatu_bse_solve", L.SOLVER_DENSE_FP64, nst, L.ptr(allv), None)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        t_fp64 = t0.elapsed_time(t1) / 1e3
+        extra["fp64_path"] = {"s_per_system": t_fp64, "solver": "FP64 build + dense FP64 eigensolve (cuSOLVER)",
+                              "speedup_mixed_vs_fp64": t_fp64 / t_step,
+                              "max_abs_dE_eV_lowest8": float(np.abs(w_mixed - allv[:nst]).max())}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, desc, threads = cpu_sample(ncell)
+        cpu = {"value": v, "unit": "s/system", "cores": threads, "kind": "port", "sample": desc}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "s/system", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16x2 (split) + fp32 accumulate, fp64 diagonal/orthogonalisation",
+                "data": "synthetic",
+                "config": {"workload": f"{WORKLOAD['model']}, Nk={ncell}x{ncell}, 2v+2c, N={N}, lowest {nst} "
+                                       "states, real-space Keldysh r0=40 eps=(1,4.5), direct only",
+                           "path": "mixed: device bands + tables + split-BF16 assembly + block Davidson",
+                           "l2": "inputs larger than L2 (K = 1.66 GB)", "parallelism": f"replicas x{world}"},
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": t_e2e, "unit": "s/system", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(gpu_launches), "clocks": clocks}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    ex.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

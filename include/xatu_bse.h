@@ -1,0 +1,201 @@
+/*
+ * xatu_bse.h -- C ABI of the B200 BSE engine.
+ *
+ * The engine replaces the hot path of Xatu's ExcitonTB:
+ *
+ *   ExcitonTB::initializeHamiltonian()         include/xatu/ExcitonTB.hpp:140
+ *   ExcitonTB::BShamiltonian() / (basis)       include/xatu/ExcitonTB.hpp:141-142
+ *   ExcitonTB::diagonalize(method, nstates)    include/xatu/ExcitonTB.hpp:143
+ *
+ * together with the pure virtuals they implement (include/xatu/Exciton.hpp:117,125-126).
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *   - Complex numbers are interleaved (re, im) doubles.
+ *   - Matrices are row-major unless stated otherwise.  The tight-binding
+ *     matrices H(R) are given per cell as [R][row][col] (an Armadillo cube
+ *     slice is column-major; a caller holding one passes its transpose, see
+ *     INTEGRATION.md).
+ *   - Units: Angstrom and eV, as in the reference.
+ *   - Every call returns a status; xatu_last_error() gives the message of the
+ *     last failing call on that context.  No call throws, exits or spins
+ *     without bound.
+ *   - A context owns one CUDA stream on the device it was created on and all
+ *     device buffers (band stacks, interaction tables, the BSE matrix).  One
+ *     context per host thread.
+ */
+#ifndef XATU_BSE_H
+#define XATU_BSE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xatu_ctx xatu_ctx;
+typedef int xatu_status;
+
+enum {
+  XATU_OK = 0,
+  XATU_ERR_INVALID = 1,        /* bad argument or inconsistent sizes (reference: std::invalid_argument) */
+  XATU_ERR_CUDA = 2,           /* a CUDA / cuSOLVER / cuBLAS call failed */
+  XATU_ERR_NOT_CONVERGED = 3,  /* an iterative solver hit its iteration or time cap */
+  XATU_ERR_STATE = 4,          /* call out of order (e.g. solve before build) */
+  XATU_ERR_ALLOC = 5,          /* device or host allocation failed */
+  XATU_ERR_UNSUPPORTED = 6,    /* valid input outside what this build supports */
+  XATU_ERR_NUMERIC = 7         /* NaN/Inf found in inputs or results */
+};
+
+enum { XATU_MODE_REALSPACE = 0, XATU_MODE_RECIPROCAL = 1 };          /* ExcitonTB::setMode */
+enum { XATU_POT_KELDYSH = 0, XATU_POT_COULOMB = 1 };                  /* ExcitonTB::selectPotential */
+enum { XATU_GAUGE_LATTICE = 0, XATU_GAUGE_ATOMIC = 1 };               /* ExcitonTB::setGauge */
+
+/* Storage/arithmetic of the assembled BSE matrix. */
+enum {
+  XATU_PREC_FP64 = 0,   /* complex128 H, FP64 arithmetic (parity mode; the reference's HBS_) */
+  XATU_PREC_MIXED = 1   /* FP64 band-energy diagonal + interaction kernel in split BF16 (hi + lo),
+                           FP32 arithmetic; the tensor-core solve path */
+};
+
+/* Solvers for xatu_bse_solve (ExcitonTB::diagonalizeRaw, ExcitonTB.cpp:930-959). */
+enum {
+  XATU_SOLVER_DENSE_FP64 = 0,  /* all eigenpairs, FP64 (the reference's "diag"); needs XATU_PREC_FP64 */
+  XATU_SOLVER_DAVIDSON = 1     /* lowest nstates; block Davidson, FP64 orthogonalisation and Rayleigh-Ritz,
+                                  H.X on tcgen05 tensor cores from the split-BF16 kernel (XATU_PREC_MIXED)
+                                  or FP64 CUDA cores (XATU_PREC_FP64) */
+};
+
+/* SystemTB inputs (System.hpp:20-40, Lattice.hpp:21-63, SystemConfiguration.hpp:13-36). */
+typedef struct {
+  int ndim;                    /* 1, 2 or 3 */
+  const double *bravais;       /* ndim x 3 */
+  int natoms;
+  const double *motif;         /* natoms x 4: x, y, z, species index */
+  int nspecies;
+  const int *norbitals;        /* orbitals per species */
+  int ncells;                  /* number of H(R) matrices */
+  const double *cells;         /* ncells x 3, R vectors */
+  const double *hamiltonian;   /* ncells x norb x norb complex, [R][row][col] */
+  const double *overlap;       /* NULL, or like hamiltonian (non-orthogonal basis, Loewdin) */
+  int filling;                 /* electrons; Fermi level band = filling - 1 */
+  int is_triangular;           /* -1: detect from H(R_0) like checkIfTriangular (utils.cpp:176-178) */
+  int is_au;                   /* energies in Hartree (scaled by 27.2 in solveBands, SystemTB.cpp:117-120) */
+} xatu_system_desc;
+
+/* ExcitonTB parameters (ExcitonTB.hpp:30-45, Exciton.hpp:29-48). */
+typedef struct {
+  int ncell;                   /* k points per axis of the full mesh (before the submesh factor) */
+  int factor;                  /* reduced-mesh factor (Lattice::reducedBrillouinZoneMesh), 1 = full mesh */
+  int nk;                      /* rows of kpoints */
+  const double *kpoints;       /* nk x 3: the exciton basis k points (Lattice::kpoints) */
+  int nmesh;                   /* rows of mesh ((ncell*factor)^ndim) */
+  const double *mesh;          /* nmesh x 3: full BZ mesh (Lattice::meshBZ); NULL = kpoints */
+  int nvalence, nconduction;
+  const int *valence_bands;    /* absolute band indices (ExcitonTB::valenceBands) */
+  const int *conduction_bands; /* absolute band indices (ExcitonTB::conductionBands) */
+  double eps_m, eps_s, r0;
+  double regularization;       /* < 1e-10 -> |a1| (ExcitonTB.cpp:803-805) */
+  double cutoff;               /* ExcitonTB::cutoff_ in units of |a1|; <= 0 -> ncell / 2.5 */
+  double Q[3];                 /* exciton centre-of-mass momentum */
+  double scissor;
+  int exchange;                /* 0 / 1 */
+  int mode;                    /* XATU_MODE_* */
+  int n_reciprocal;            /* reciprocal vectors per axis (ExcitonTB::nReciprocalVectors) */
+  int potential;               /* XATU_POT_* for the direct term (real space) */
+  int exchange_potential;      /* XATU_POT_* for the exchange term (real space) */
+  int gauge;                   /* XATU_GAUGE_* */
+} xatu_exciton_desc;
+
+/* ------------------------------------------------------------------ context */
+xatu_status xatu_ctx_create(xatu_ctx **ctx, int device);
+xatu_status xatu_ctx_destroy(xatu_ctx *ctx);
+const char *xatu_last_error(const xatu_ctx *ctx);
+/* Run the context's work on an external stream (cudaStream_t passed as void*; NULL = own stream). */
+xatu_status xatu_ctx_set_stream(xatu_ctx *ctx, void *stream);
+int xatu_abi_version(void);
+
+/* ------------------------------------------------------------------ inputs */
+/* Copies the SystemTB arrays (the constructor SystemTB(SystemConfiguration), SystemTB.cpp:29-31). */
+xatu_status xatu_system_upload(xatu_ctx *ctx, const xatu_system_desc *sys);
+/* Copies the exciton parameters, builds the e-h basis (Exciton::createBasis, Exciton.tpp:128-147), the
+   real-space cell list (Lattice::truncateSupercell, Lattice.cpp:320-341) and the reciprocal-vector list
+   (Lattice::truncateReciprocalSupercell, Lattice.cpp:349-370).  ExcitonTB::initializeHamiltonian's guards
+   (ExcitonTB.cpp:794-815) apply. */
+xatu_status xatu_exciton_set(xatu_ctx *ctx, const xatu_exciton_desc *exc);
+
+/* ------------------------------------------------------------------ initializeResultsH0 (ExcitonTB.cpp:707-787) */
+/* Band solve at every k (and k+Q) on the device: Bloch H(k) (SystemTB.cpp:60-75), Hermitian eigensolve
+   (SystemTB.cpp:113-125), fixGlobalPhase (ExcitonTB.cpp:673-683), band selection. */
+xatu_status xatu_bands_compute(xatu_ctx *ctx);
+/* Alternative: caller-supplied band stacks (gauge-controlled parity).  eigval: nk x nb,
+   eigvec: nk x nb x norb complex (band b of k at [k][b][:]); nb = nvalence + nconduction, valence first.
+   eigvalQ/eigvecQ may be NULL when Q = 0. */
+xatu_status xatu_bands_upload(xatu_ctx *ctx, const double *eigval, const double *eigvec,
+                              const double *eigvalQ, const double *eigvecQ);
+xatu_status xatu_bands_download(xatu_ctx *ctx, double *eigval, double *eigvec, double *eigvalQ,
+                                double *eigvecQ);
+/* Interaction tables: motif lattice Fourier transform V_ab(q) over the mesh (ExcitonTB.cpp:438-476, :761-786)
+   or, in reciprocal mode, the G-summed kernel (ExcitonTB.cpp:410-426, :562-621). */
+xatu_status xatu_interaction_build(xatu_ctx *ctx);
+/* nmesh x na x na complex, and na x na complex (exchange at Q). */
+xatu_status xatu_motif_ft_download(xatu_ctx *ctx, double *ft_stack, double *ft_Q);
+
+/* ------------------------------------------------------------------ BShamiltonian (ExcitonTB.cpp:840-921) */
+/* Runs the band solve and interaction tables if they are not current, then assembles H on the device. */
+xatu_status xatu_bse_build(xatu_ctx *ctx, int precision);
+xatu_status xatu_bse_dim(const xatu_ctx *ctx, int64_t *n);
+/* Full Hermitian H, row-major N x N complex (FP64 build), or the mixed build expanded to complex128
+   (diagonal band term + split-BF16 kernel). */
+xatu_status xatu_bse_copy_to_host(xatu_ctx *ctx, double *H);
+/* Device pointer and layout of the assembled matrix (row-major complex128 for FP64; for MIXED the two
+   split-BF16 planes hi and lo, each N x N complex bf16, and the FP64 diagonal). */
+xatu_status xatu_bse_device_buffers(xatu_ctx *ctx, void **h_or_hi, void **lo, void **diag);
+
+/* ------------------------------------------------------------------ diagonalize (ExcitonTB.cpp:930-972) */
+/* DAVIDSON: eigval receives nstates doubles (ascending).  DENSE_FP64: eigval receives all N eigenvalues
+   (ascending), like arma::eig_sym.  eigvec: NULL, or the eigenvectors of the lowest nstates states
+   (all N when nstates <= 0 with DENSE_FP64) as N x nstates complex, column s = state s, column-major
+   (Armadillo layout). */
+xatu_status xatu_bse_solve(xatu_ctx *ctx, int solver, int nstates, double *eigval, double *eigvec);
+/* Davidson controls: residual tolerance (eV), iteration cap, block size (0 = automatic). */
+xatu_status xatu_davidson_config(xatu_ctx *ctx, double tol, int max_iter, int block);
+/* Iterations used by the last Davidson solve. */
+xatu_status xatu_davidson_stats(const xatu_ctx *ctx, int *iterations, double *max_residual);
+/* Kernel of H.X for the mixed build: 0 automatic (tcgen05 tensor cores when the layout allows), 1 CUDA cores,
+   2 tensor cores.  No reference counterpart (the reference multiplies dense Armadillo matrices, davidson.cpp:31-37). */
+xatu_status xatu_hx_backend(xatu_ctx *ctx, int backend);
+/* Y = H X for nvec host vectors with the current build (X, Y: N x nvec complex, column-major); the product the
+   Davidson iterations use. */
+xatu_status xatu_kernel_matvec(xatu_ctx *ctx, int nvec, const double *X, double *Y);
+
+/* ------------------------------------------------------------------ instrumentation */
+/* Device milliseconds of the last run of each stage: [0] bands, [1] interaction tables, [2] assembly,
+   [3] solve.  Measured with CUDA events on the context's stream. */
+xatu_status xatu_stage_times(const xatu_ctx *ctx, float *ms4);
+/* Device time of one kernel family measured with CUDA events on the context's stream: which = 0 the BSE
+   assembly (last build), 1 the K.X products of the last Davidson solve.  *path: 1 CUDA cores, 2 tcgen05. */
+xatu_status xatu_kernel_stats(const xatu_ctx *ctx, int which, int64_t *launches, double *total_ms, int *path);
+/* Number of engine kernels launched on this context since creation. */
+xatu_status xatu_kernel_launches(const xatu_ctx *ctx, int64_t *count);
+
+/* ------------------------------------------------------------------ geometry helpers (host, no device work) */
+/* Lattice::calculateReciprocalLattice (Lattice.cpp:56-80): out ndim x 3. */
+xatu_status xatu_reciprocal_lattice(int ndim, const double *bravais, double *recip);
+/* Lattice::brillouinZoneMesh (Lattice.cpp:140-162): out n^ndim x 3. */
+xatu_status xatu_mesh_mp(int ndim, const double *recip, int n, double *kpoints);
+/* Lattice::reducedBrillouinZoneMesh (Lattice.cpp:172-197): submesh n^ndim x 3 (mesh: xatu_mesh_mp(n*factor)). */
+xatu_status xatu_mesh_reduced(int ndim, const double *recip, int n, int factor, double *kpoints);
+/* Lattice::findEquivalentPointBZ (Lattice.cpp:251-279) for a batch of points: index into the n_eff mesh. */
+xatu_status xatu_equivalent_points(int ndim, const double *recip, int n_eff, int npts, const double *k,
+                                   int *index);
+/* Lattice::truncateSupercell (Lattice.cpp:320-341): count only when cells == NULL. */
+xatu_status xatu_truncate_supercell(int ndim, const double *bravais, int ncell, double radius, int *count,
+                                    double *cells);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XATU_BSE_H */

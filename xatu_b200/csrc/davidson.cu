@@ -1,0 +1,581 @@
+// Block Davidson for the lowest exciton states of the BSE matrix, kept on
+// the device (replaces davidson_method, davidson.cpp:5-60, and the dense
+// eigensolve when only a few states are wanted).
+//
+// Design (not the reference's algorithm; it converges to the same lowest
+// eigenpairs):
+//   * start vectors: unit vectors at the smallest diagonal entries of H
+//     (the reference starts from the first identity columns, davidson.cpp:19);
+//   * H.V: mixed build -> diag(E) V in FP64 plus K V with K = K_hi + K_lo
+//     (split BF16, FP32 accumulation); FP64 build -> ZGEMM on the FP64 matrix;
+//   * Rayleigh-Ritz in FP64: T = V^H (H V), Jacobi eigensolve on the device;
+//   * residuals r = H u - theta u in FP64, per-row diagonal preconditioner
+//     t = r / (theta - H_ii) (the reference divides by H_jj of the state
+//     index j, davidson.cpp:36-40);
+//   * FP64 orthogonalisation: two passes of block classical Gram-Schmidt
+//     against the basis, then pivoted Cholesky-QR (twice) inside the block;
+//   * thick restart on the lowest `block` Ritz vectors when the basis is full;
+//   * caps on iterations and wall time -> XATU_ERR_NOT_CONVERGED.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "engine.h"
+#include "jacobi.cuh"
+
+#define DAV_EIGH_THREADS 512
+#define DAV_MAX_BASIS 112
+
+// ---------------------------------------------------------------- kernels
+__global__ void dav_diag_mixed_kernel(const __nv_bfloat162* __restrict__ Khi, const __nv_bfloat162* __restrict__ Klo,
+                                      const double* __restrict__ d, long long N, long long ldk, double* __restrict__ out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  out[i] = d[i] + (double)__bfloat162float(Khi[i * ldk + i].x) + (double)__bfloat162float(Klo[i * ldk + i].x);
+}
+
+__global__ void dav_diag_fp64_kernel(const cd* __restrict__ H, long long N, double* __restrict__ out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  out[i] = H[i * N + i].x;
+}
+
+// V[:, col0 + s] = e_{idx[s]}
+__global__ void dav_unit_vectors_kernel(cd* V, long long N, int col0, const int* idx, int nvec) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * nvec) return;
+  const int s = (int)(t / N);
+  const long long i = t - (long long)s * N;
+  V[(long long)(col0 + s) * N + i] = mk(i == idx[s] ? 1.0 : 0.0, 0.0);
+}
+
+// X (row-major N x nv, complex float) <- V[:, col0 : col0 + nv]
+__global__ void dav_gather_f32_kernel(const cd* __restrict__ V, long long N, int col0, int nv, float2* __restrict__ X) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * nv) return;
+  const long long i = t / nv;
+  const int s = (int)(t - i * nv);
+  const cd v = V[(long long)(col0 + s) * N + i];
+  X[t] = make_float2((float)v.x, (float)v.y);
+}
+
+// W[:, col0 + s] = Y[:, s] + d .* V[:, col0 + s]   (the FP64 band-energy diagonal)
+__global__ void dav_finish_w_kernel(const float2* __restrict__ Y, const double* __restrict__ d,
+                                    const cd* __restrict__ V, long long N, int col0, int nv, cd* __restrict__ W) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * nv) return;
+  const long long i = t / nv;
+  const int s = (int)(t - i * nv);
+  const float2 y = Y[t];
+  const long long o = (long long)(col0 + s) * N + i;
+  const cd v = V[o];
+  W[o] = mk((double)y.x + d[i] * v.x, (double)y.y + d[i] * v.y);
+}
+
+// T (column-major, ld) : fill T[m0:m, 0:m0] = conj(T[0:m0, m0:m])^T and make the new block Hermitian.
+__global__ void dav_hermitize_kernel(cd* T, int ld, int m, int m0) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nnew = m - m0;
+  if (t >= nnew * m) return;
+  const int c = m0 + t / m;   // column in the new block
+  const int r = t % m;        // row
+  if (r < m0) {
+    const cd v = T[r + (long long)c * ld];
+    T[c + (long long)r * ld] = conj(v);
+  } else if (r < c) {
+    const cd a = T[r + (long long)c * ld], b = T[c + (long long)r * ld];
+    const cd h = mk(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    T[r + (long long)c * ld] = h;
+    T[c + (long long)r * ld] = conj(h);
+  } else if (r == c) {
+    T[r + (long long)c * ld].y = 0.0;
+  }
+}
+
+// T = diag(theta[0:k])
+__global__ void dav_set_diag_kernel(cd* T, int ld, int k, const double* theta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= k * k) return;
+  const int r = t % k, c = t / k;
+  T[r + (long long)c * ld] = mk(r == c ? theta[r] : 0.0, 0.0);
+}
+
+// One-block eigensolve of T (m x m, column-major ld) -> theta ascending, Y column-major ld (sorted).
+__global__ void __launch_bounds__(DAV_EIGH_THREADS)
+dav_small_eigh_kernel(const cd* __restrict__ T, int ld, int m, double* __restrict__ theta, cd* __restrict__ Y,
+                      cd* __restrict__ Vscratch, int max_sweeps, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lda = m + 1;
+  cd* A = reinterpret_cast<cd*>(smem_raw);
+  JacobiRot* rot = reinterpret_cast<JacobiRot*>(A + (size_t)m * lda);
+  double* scratch = reinterpret_cast<double*>(rot + (m / 2 + 2));
+  int* perm = reinterpret_cast<int*>(scratch + 64);
+  BlockGroup g;
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int r = t / m, c = t - r * m;
+    A[r * lda + c] = T[r + (long long)c * ld];
+  }
+  __syncthreads();
+  const int sweeps = jacobi_eigh(g, A, lda, Vscratch, m, m, rot, scratch, max_sweeps, 1e-15);
+  if (sweeps > max_sweeps && threadIdx.x == 0) atomicOr(status, XATU_DEVERR_NOCONV);
+  jacobi_sort(g, A, lda, m, perm);
+  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+    const int c = t / m, r = t - c * m;   // column c of the sorted output
+    Y[r + (long long)c * ld] = Vscratch[r * m + perm[c]];
+  }
+  for (int c = threadIdx.x; c < m; c += blockDim.x) theta[c] = A[perm[c] * lda + perm[c]].x;
+}
+
+// R[:, s] = WU[:, s] - theta[s] U[:, s]; norms[s] = ||R[:, s]||  (one block per column)
+__global__ void dav_residual_kernel(const cd* __restrict__ U, const cd* __restrict__ WU, const double* __restrict__ theta,
+                                    long long N, cd* __restrict__ R, double* __restrict__ norms) {
+  const int s = blockIdx.x;
+  const double th = theta[s];
+  double acc = 0.0;
+  for (long long i = threadIdx.x; i < N; i += blockDim.x) {
+    const long long o = (long long)s * N + i;
+    const cd u = U[o], w = WU[o];
+    const cd r = mk(w.x - th * u.x, w.y - th * u.y);
+    R[o] = r;
+    acc += nrm2(r);
+  }
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s2 += red[w];
+    norms[s] = sqrt(s2);
+  }
+}
+
+// V[:, col0 + j] = R[:, sel[j]] / (theta[sel[j]] - diagH)
+__global__ void dav_precondition_kernel(const cd* __restrict__ R, const double* __restrict__ theta,
+                                        const double* __restrict__ diagH, const int* __restrict__ sel, int nsel,
+                                        long long N, cd* __restrict__ V, int col0) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * nsel) return;
+  const int j = (int)(t / N);
+  const long long i = t - (long long)j * N;
+  const int s = sel[j];
+  double den = theta[s] - diagH[i];
+  if (fabs(den) < 1e-8) den = (den < 0 ? -1e-8 : 1e-8);
+  const cd r = R[(long long)s * N + i];
+  V[(long long)(col0 + j) * N + i] = mk(r.x / den, r.y / den);
+}
+
+// ---------------------------------------------------------------- host helpers
+struct Z {
+  double x, y;
+};
+
+static const cuDoubleComplex kOne = {1.0, 0.0}, kZero = {0.0, 0.0}, kMinusOne = {-1.0, 0.0};
+
+// Pivoted Cholesky of the Hermitian Gram matrix G (n x n, column-major) ->
+// S (n x k, column-major) with S^H G S = I over the kept directions.  Columns
+// whose remaining norm falls below rel * max diag are dropped.
+static int gram_to_orthonormalizer(const std::vector<Z>& G, int n, double rel, std::vector<Z>& S) {
+  // Modified Gram-Schmidt in the G inner product, column by column.
+  std::vector<Z> B(n * n, Z{0, 0});  // columns of B are coefficient vectors
+  std::vector<int> kept;
+  double maxd = 0;
+  for (int i = 0; i < n; i++) maxd = std::max(maxd, G[i + i * n].x);
+  auto gdot = [&](const Z* a, const Z* b) {  // a^H G b
+    Z s{0, 0};
+    for (int r = 0; r < n; r++) {
+      Z gb{0, 0};
+      for (int c = 0; c < n; c++) {
+        const Z g = G[r + c * n];
+        gb.x += g.x * b[c].x - g.y * b[c].y;
+        gb.y += g.x * b[c].y + g.y * b[c].x;
+      }
+      s.x += a[r].x * gb.x + a[r].y * gb.y;
+      s.y += a[r].x * gb.y - a[r].y * gb.x;
+    }
+    return s;
+  };
+  std::vector<Z> cols;
+  for (int j = 0; j < n; j++) {
+    std::vector<Z> v(n, Z{0, 0});
+    v[j] = Z{1, 0};
+    for (int pass = 0; pass < 2; pass++)
+      for (size_t q = 0; q < cols.size() / n; q++) {
+        const Z* u = &cols[q * n];
+        const Z c = gdot(u, v.data());
+        for (int r = 0; r < n; r++) {
+          v[r].x -= c.x * u[r].x - c.y * u[r].y;
+          v[r].y -= c.x * u[r].y + c.y * u[r].x;
+        }
+      }
+    const double nn = gdot(v.data(), v.data()).x;
+    if (nn <= rel * maxd || nn <= 0) continue;
+    const double f = 1.0 / std::sqrt(nn);
+    for (int r = 0; r < n; r++) {
+      v[r].x *= f;
+      v[r].y *= f;
+    }
+    cols.insert(cols.end(), v.begin(), v.end());
+  }
+  S = cols;
+  return (int)(cols.size() / n);
+}
+
+// Bt operand of the tensor-core product (hx_tc.cu) from V[:, col0 : col0 + b]:
+//   rows [0, bp):   Re X at 2j, -Im X at 2j+1;   rows [bp, 2bp): Im X at 2j, Re X at 2j+1
+// (bp = b rounded up to 8; padding rows are zero), split into BF16 hi + lo.
+__global__ void dav_build_bt_kernel(const cd* __restrict__ V, long long N, int col0, int b, int bp, long long ldb,
+                                    __nv_bfloat16* __restrict__ Bhi, __nv_bfloat16* __restrict__ Blo) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * bp) return;
+  const int s = (int)(t / N);
+  const long long j = t - (long long)s * N;
+  float re = 0.f, im = 0.f;
+  if (s < b) {
+    const cd v = V[(long long)(col0 + s) * N + j];
+    re = (float)v.x;
+    im = (float)v.y;
+  }
+  const float vals[4] = {re, -im, im, re};
+  const long long off[4] = {(long long)s * ldb + 2 * j, (long long)s * ldb + 2 * j + 1,
+                            (long long)(bp + s) * ldb + 2 * j, (long long)(bp + s) * ldb + 2 * j + 1};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(vals[q]);
+    Bhi[off[q]] = h;
+    Blo[off[q]] = __float2bfloat16_rn(vals[q] - __bfloat162float(h));
+  }
+}
+
+// W[:, col0 + s] = (Y_re[:, s], Y_im[:, s]) + d .* V[:, col0 + s]; Y column-major N x 2bp.
+__global__ void dav_finish_w_tc_kernel(const float* __restrict__ Y, const double* __restrict__ d,
+                                       const cd* __restrict__ V, long long N, int col0, int b, int bp,
+                                       cd* __restrict__ W) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= N * b) return;
+  const int s = (int)(t / N);
+  const long long i = t - (long long)s * N;
+  const long long o = (long long)(col0 + s) * N + i;
+  const cd v = V[o];
+  W[o] = mk((double)Y[(long long)s * N + i] + d[i] * v.x, (double)Y[(long long)(bp + s) * N + i] + d[i] * v.y);
+}
+
+static bool tc_usable(const xatu_ctx* ctx) {
+  if (ctx->hx_backend == 1) return false;
+  return (ctx->ldk % 4) == 0;
+}
+
+xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
+  cd* V = ctx->dv_V.as<cd>();
+  cd* W = ctx->dv_W.as<cd>();
+  const int threads = 256;
+  if (ctx->built_prec == XATU_PREC_FP64) {
+    static const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0};
+    cublasStatus_t bs = cublasZgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)N, nv, (int)N, &one,
+                                    ctx->d_H.as<cuDoubleComplex>(), (int)N,
+                                    reinterpret_cast<cuDoubleComplex*>(V + (long long)col0 * N), (int)N, &zero,
+                                    reinterpret_cast<cuDoubleComplex*>(W + (long long)col0 * N), (int)N);
+    if (bs != CUBLAS_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZgemm (H.V) failed");
+    return XATU_OK;
+  }
+  if (tc_usable(ctx)) {
+    const long long ldb = (2 * N + 7) / 8 * 8;
+    for (int c = 0; c < nv; c += 32) {
+      const int b = std::min(32, nv - c);
+      const int bp = (b + 7) / 8 * 8;
+      const int ng = 2 * bp;
+      XATU_CK(ctx->dv_Bop.ensure((size_t)64 * ldb * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Blo.ensure((size_t)64 * ldb * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Yf.ensure((size_t)N * 64 * sizeof(float)));
+      const long long tb = N * bp;
+      dav_build_bt_kernel<<<(int)((tb + threads - 1) / threads), threads, 0, ctx->stream>>>(
+          V, N, col0 + c, b, bp, ldb, ctx->dv_Bop.as<__nv_bfloat16>(), ctx->dv_Blo.as<__nv_bfloat16>());
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+      XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+      XATU_CK(xatu_launch_hx_tc(ctx->d_Khi.p, ctx->d_Klo.p, N, ctx->ldk, ctx->dv_Bop.p, ctx->dv_Blo.p, ldb, ng,
+                                ctx->dv_Yf.as<float>(), ctx->d_status.as<int>(), ctx->num_sms, ctx->stream));
+      XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+      XATU_CK(cudaEventSynchronize(ctx->ev[9]));
+      {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]);
+        ctx->hx_ms += ms;
+        ctx->hx_calls++;
+        ctx->hx_last_path = 2;
+      }
+      ctx->launches++;
+      const long long tw = N * b;
+      dav_finish_w_tc_kernel<<<(int)((tw + threads - 1) / threads), threads, 0, ctx->stream>>>(
+          ctx->dv_Yf.as<float>(), ctx->d_diag.as<double>(), V, N, col0 + c, b, bp, W);
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+    }
+    return XATU_OK;
+  }
+  XATU_CK(ctx->dv_X.ensure((size_t)N * 32 * sizeof(float2)));
+  XATU_CK(ctx->dv_Yf.ensure((size_t)N * 64 * sizeof(float)));
+  for (int c = 0; c < nv; c += 32) {
+    const int b = std::min(32, nv - c);
+    const long long tot = N * b;
+    const int blocks = (int)((tot + threads - 1) / threads);
+    dav_gather_f32_kernel<<<blocks, threads, 0, ctx->stream>>>(V, N, col0 + c, b, ctx->dv_X.as<float2>());
+    ctx->launches++;
+    XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+    XATU_CK(xatu_launch_hx_cuda_core(ctx->d_Khi.as<__nv_bfloat162>(), ctx->d_Klo.as<__nv_bfloat162>(), ctx->ldk,
+                                     ctx->dv_X.as<float2>(), ctx->dv_Yf.as<float2>(), N, b, ctx->stream));
+    XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+    XATU_CK(cudaEventSynchronize(ctx->ev[9]));
+    {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]);
+      ctx->hx_ms += ms;
+      ctx->hx_calls++;
+      ctx->hx_last_path = 1;
+    }
+    ctx->launches++;
+    dav_finish_w_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->dv_Yf.as<float2>(), ctx->d_diag.as<double>(), V, N,
+                                                             col0 + c, b, W);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
+  }
+  return XATU_OK;
+}
+
+static xatu_status zgemm(xatu_ctx* ctx, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                         const cuDoubleComplex* alpha, const cd* A, int lda, const cd* B, int ldb,
+                         const cuDoubleComplex* beta, cd* C, int ldc) {
+  cublasStatus_t s = cublasZgemm(ctx->blas, ta, tb, m, n, k, alpha, reinterpret_cast<const cuDoubleComplex*>(A), lda,
+                                 reinterpret_cast<const cuDoubleComplex*>(B), ldb, beta,
+                                 reinterpret_cast<cuDoubleComplex*>(C), ldc);
+  if (s != CUBLAS_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZgemm failed");
+  return XATU_OK;
+}
+
+#define XATU_TRY(x)                  \
+  do {                               \
+    xatu_status s__ = (x);           \
+    if (s__ != XATU_OK) return s__;  \
+  } while (0)
+
+// Orthonormalise V[:, m : m + nsel] against V[:, 0 : m] and within itself.
+// Returns the number of vectors kept (moved to V[:, m : m + kept]).
+static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int nsel, int* kept) {
+  cd* V = ctx->dv_V.as<cd>();
+  cd* tblk = V + (long long)m * N;
+  cd* C = ctx->dv_G.as<cd>();
+  const int ldC = DAV_MAX_BASIS;
+  for (int pass = 0; pass < 2; pass++) {
+    if (m > 0) {
+      XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nsel, (int)N, &kOne, V, (int)N, tblk, (int)N, &kZero, C, ldC));
+      XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nsel, m, &kMinusOne, V, (int)N, C, ldC, &kOne, tblk,
+                     (int)N));
+    }
+  }
+  int cur = nsel;
+  for (int pass = 0; pass < 2 && cur > 0; pass++) {
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, cur, cur, (int)N, &kOne, tblk, (int)N, tblk, (int)N, &kZero, C, ldC));
+    std::vector<Z> Gh((size_t)cur * cur), Gc((size_t)ldC * cur);
+    XATU_CK(cudaMemcpyAsync(Gc.data(), C, sizeof(Z) * (size_t)ldC * cur, cudaMemcpyDeviceToHost, ctx->stream));
+    XATU_CK(cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < cur; c++)
+      for (int r = 0; r < cur; r++) Gh[r + (size_t)c * cur] = Gc[r + (size_t)c * ldC];
+    std::vector<Z> S;
+    const int k = gram_to_orthonormalizer(Gh, cur, pass == 0 ? 1e-20 : 1e-24, S);
+    if (k == 0) {
+      cur = 0;
+      break;
+    }
+    // tmp = tblk * S  (N x k), then copy back into tblk
+    XATU_CK(ctx->dv_small.ensure(sizeof(Z) * (size_t)cur * k + 64));
+    XATU_CK(cudaMemcpyAsync(ctx->dv_small.p, S.data(), sizeof(Z) * (size_t)cur * k, cudaMemcpyHostToDevice, ctx->stream));
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, k, cur, &kOne, tblk, (int)N, ctx->dv_small.as<cd>(), cur,
+                   &kZero, ctx->dv_tmp.as<cd>(), (int)N));
+    XATU_CK(cudaMemcpyAsync(tblk, ctx->dv_tmp.p, sizeof(cd) * (size_t)N * k, cudaMemcpyDeviceToDevice, ctx->stream));
+    cur = k;
+  }
+  *kept = cur;
+  return XATU_OK;
+}
+
+xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec) {
+  const long long N = ctx->N;
+  if (!ctx->blas) {
+    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cublasCreate failed");
+  }
+  cublasSetStream(ctx->blas, ctx->stream);
+  cublasSetPointerMode(ctx->blas, CUBLAS_POINTER_MODE_HOST);
+  const bool mixed = ctx->built_prec == XATU_PREC_MIXED;
+  int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, 2 * nstates);
+  bsz = std::max(bsz, nstates);
+  bsz = (int)std::min<long long>(bsz, N);
+  int mmax = (int)std::min<long long>(N, std::min(DAV_MAX_BASIS, 4 * bsz));
+  if (mmax < bsz + 1 && N > bsz) mmax = std::min<long long>(N, bsz + 1);
+  if (bsz > DAV_MAX_BASIS / 2 && N > DAV_MAX_BASIS)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "Davidson block too large (nstates > 56)");
+  const double tol = ctx->dav_tol > 0 ? ctx->dav_tol : (mixed ? 1e-4 : 1e-6);
+  const size_t vbytes = (size_t)N * mmax * sizeof(cd);
+  XATU_CK(ctx->dv_V.ensure(vbytes));
+  XATU_CK(ctx->dv_W.ensure(vbytes));
+  XATU_CK(ctx->dv_U.ensure((size_t)N * bsz * sizeof(cd)));
+  XATU_CK(ctx->dv_Y.ensure((size_t)N * bsz * sizeof(cd)));   // WU
+  XATU_CK(ctx->dv_R.ensure((size_t)N * bsz * sizeof(cd)));
+  XATU_CK(ctx->dv_tmp.ensure((size_t)N * mmax * sizeof(cd)));
+  XATU_CK(ctx->dv_T.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd) * 2 + 4096));
+  XATU_CK(ctx->dv_G.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd)));
+  XATU_CK(ctx->dv_diagH.ensure((size_t)N * sizeof(double)));
+  XATU_CK(ctx->dv_norm.ensure(4096 * sizeof(double)));
+  cd* V = ctx->dv_V.as<cd>();
+  cd* W = ctx->dv_W.as<cd>();
+  cd* U = ctx->dv_U.as<cd>();
+  cd* WU = ctx->dv_Y.as<cd>();
+  cd* R = ctx->dv_R.as<cd>();
+  const int ldT = DAV_MAX_BASIS;
+  cd* T = ctx->dv_T.as<cd>();
+  cd* Yr = T + (size_t)ldT * ldT;                       // Ritz coefficient matrix (ldT x ldT)
+  double* theta = ctx->dv_norm.as<double>();            // [0, 256)
+  double* norms = theta + 256;                          // [256, 512)
+  int* sel_dev = reinterpret_cast<int*>(theta + 512);   // ints
+  cd* Vscratch = ctx->dv_G.as<cd>();                    // Jacobi eigenvectors (row-major m x m)
+  double* diagH = ctx->dv_diagH.as<double>();
+  const int threads = 256;
+  // diagonal of H
+  {
+    const int blocks = (int)((N + threads - 1) / threads);
+    if (mixed)
+      dav_diag_mixed_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->d_Khi.as<__nv_bfloat162>(),
+                                                                 ctx->d_Klo.as<__nv_bfloat162>(),
+                                                                 ctx->d_diag.as<double>(), N, ctx->ldk, diagH);
+    else
+      dav_diag_fp64_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->d_H.as<cd>(), N, diagH);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
+  }
+  std::vector<double> hdiag(N);
+  XATU_CK(cudaMemcpyAsync(hdiag.data(), diagH, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  XATU_CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> order(N);
+  std::iota(order.begin(), order.end(), 0);
+  std::partial_sort(order.begin(), order.begin() + bsz, order.end(),
+                    [&](int a, int b) { return hdiag[a] < hdiag[b] || (hdiag[a] == hdiag[b] && a < b); });
+  XATU_CK(cudaMemcpyAsync(sel_dev, order.data(), bsz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  {
+    const long long tot = N * bsz;
+    dav_unit_vectors_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(V, N, 0, sel_dev, bsz);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
+  }
+  // the small eigensolver's shared memory
+  const size_t eigh_smem_max = (size_t)DAV_MAX_BASIS * (DAV_MAX_BASIS + 1) * sizeof(cd) +
+                               (DAV_MAX_BASIS / 2 + 2) * sizeof(JacobiRot) + 64 * sizeof(double) +
+                               (DAV_MAX_BASIS + 1) * sizeof(int);
+  XATU_CK(cudaFuncSetAttribute(dav_small_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigh_smem_max));
+
+  int m = 0, nnew = bsz;
+  int it = 0;
+  bool converged = false;
+  std::vector<double> h_theta(ldT), h_norm(bsz);
+  const auto t_start = std::chrono::steady_clock::now();
+  const double wall_cap_s = 300.0;
+  ctx->dav_iters = 0;
+  ctx->dav_maxres = 0;
+  ctx->hx_calls = 0;
+  ctx->hx_ms = 0;
+  for (it = 0; it < ctx->dav_max_iter; it++) {
+    // 1. W for the new block
+    XATU_TRY(xatu_apply_h(ctx, N, m, nnew));
+    const int m0 = m;
+    m += nnew;
+    // 2. new columns of T = V^H W
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nnew, (int)N, &kOne, V, (int)N, W + (long long)m0 * N, (int)N,
+                   &kZero, T + (long long)m0 * ldT, ldT));
+    {
+      const int tot = nnew * m;
+      dav_hermitize_kernel<<<(tot + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, m0);
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+    }
+    // 3. Rayleigh-Ritz
+    {
+      const size_t smem = (size_t)m * (m + 1) * sizeof(cd) + (m / 2 + 2) * sizeof(JacobiRot) + 64 * sizeof(double) +
+                          (m + 1) * sizeof(int);
+      dav_small_eigh_kernel<<<1, DAV_EIGH_THREADS, smem, ctx->stream>>>(T, ldT, m, theta, Yr, Vscratch, 60,
+                                                                         ctx->d_status.as<int>());
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+    }
+    const int nritz = std::min(bsz, m);
+    // 4. Ritz vectors and their images
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, V, (int)N, Yr, ldT, &kZero, U, (int)N));
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, W, (int)N, Yr, ldT, &kZero, WU, (int)N));
+    // 5. residuals
+    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(U, WU, theta, N, R, norms);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
+    XATU_CK(cudaMemcpyAsync(h_theta.data(), theta, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    XATU_CK(cudaMemcpyAsync(h_norm.data(), norms, nritz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    int st = 0;
+    XATU_CK(cudaMemcpyAsync(&st, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    XATU_CK(cudaStreamSynchronize(ctx->stream));
+    if (st) {
+      cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream);
+      return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz Jacobi did not converge");
+    }
+    double maxres = 0;
+    for (int s = 0; s < nstates; s++) maxres = std::max(maxres, h_norm[s]);
+    for (int s = 0; s < nritz; s++)
+      if (!std::isfinite(h_norm[s]) || !std::isfinite(h_theta[s]))
+        return xatu_fail(ctx, XATU_ERR_NUMERIC, "Davidson: non-finite Ritz value or residual");
+    ctx->dav_iters = it + 1;
+    ctx->dav_maxres = maxres;
+    if (maxres < tol || m >= N) {
+      converged = true;
+      break;
+    }
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (el > wall_cap_s) break;
+    // 6. correction targets: unconverged among the kept Ritz pairs
+    std::vector<int> sel;
+    for (int s = 0; s < nritz; s++)
+      if (h_norm[s] >= tol) sel.push_back(s);
+    int nsel = (int)sel.size();
+    // 7. thick restart
+    if (m + nsel > mmax) {
+      XATU_CK(cudaMemcpyAsync(V, U, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
+      XATU_CK(cudaMemcpyAsync(W, WU, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
+      dav_set_diag_kernel<<<(nritz * nritz + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, nritz, theta);
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+      m = nritz;
+      if (m + nsel > mmax) nsel = mmax - m;
+    }
+    if (nsel <= 0) break;
+    XATU_CK(cudaMemcpyAsync(sel_dev, sel.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    {
+      const long long tot = N * nsel;
+      dav_precondition_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(
+          R, theta, diagH, sel_dev, nsel, N, V, m);
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
+    }
+    int kept = 0;
+    XATU_TRY(orthonormalize_block(ctx, N, m, nsel, &kept));
+    if (kept == 0) break;
+    nnew = kept;
+  }
+  // results
+  std::copy(h_theta.begin(), h_theta.begin() + nstates, eigval);
+  if (eigvec)
+    XATU_CK(cudaMemcpyAsync(eigvec, U, sizeof(cd) * (size_t)N * nstates, cudaMemcpyDeviceToHost, ctx->stream));
+  XATU_CK(cudaStreamSynchronize(ctx->stream));
+  if (!converged) {
+    char buf[160];
+    snprintf(buf, sizeof(buf), "Davidson: not converged after %d iterations (max residual %.3e, tol %.1e)",
+             ctx->dav_iters, ctx->dav_maxres, tol);
+    return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, buf);
+  }
+  return XATU_OK;
+}

@@ -1,0 +1,126 @@
+// Internal state of an engine context and the launchers shared between the
+// translation units of libxatu_bse.so.  Not part of the public ABI.
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/xatu_bse.h"
+#include "common.cuh"
+
+// A device allocation that only grows.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct xatu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  std::string err;
+  long long launches = 0;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  cudaEvent_t ev[10] = {};
+  float stage_ms[4] = {0, 0, 0, 0};
+
+  // ---------------- system
+  bool has_system = false;
+  int ndim = 0, natoms = 0, norb = 0, nR = 0, filling = 0;
+  bool triangular = false, is_au = false, has_overlap = false;
+  std::vector<double> bravais, recip, motif, cellsR, inv_gram;
+  std::vector<int> orb_off;
+  double a1 = 0, b1 = 0, area = 0;
+  DBuf d_motif, d_orboff, d_cellsR, d_HR, d_SR;
+
+  // ---------------- exciton
+  bool has_exciton = false;
+  int ncell = 0, factor = 1, n_eff = 0, nk = 0, nmesh = 0, nv = 0, nc = 0, nb = 0;
+  long long N = 0;
+  long long ldk = 0;          // row pitch of the mixed planes (N rounded up to 4)
+  std::vector<int> band_list;
+  double eps_m = 1, eps_s = 1, r0 = 1, regularization = 0, cutoff = 0, scissor = 0;
+  double Q[3] = {0, 0, 0};
+  bool qnonzero = false;
+  int exchange = 0, mode = 0, n_recip = 1, potential = 0, exchange_potential = 0, gauge = 0;
+  double total_cells = 1;
+  std::vector<double> kpoints, mesh, cells, G;
+  std::vector<int> kgrid;
+  bool kgrid_ok = false;
+  int rt_len[3] = {1, 1, 1}, rt_span[3] = {0, 0, 0};
+  long long rt_entries = 1;
+  DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid;
+
+  // ---------------- derived device data
+  bool bands_ok = false, tables_ok = false;
+  int built_prec = -1;
+  DBuf d_eigval, d_eigvec, d_eigvalQ, d_eigvecQ;
+  DBuf d_pairs, d_vtab, d_vtabX, d_table, d_VX, d_exL, d_exR;
+  DBuf d_H, d_Khi, d_Klo, d_diag, d_status;
+  DBuf d_work;       // solver scratch
+  int last_assembly_path = -1;
+
+  // ---------------- Davidson
+  double dav_tol = 0.0;      // 0: default per precision
+  int dav_max_iter = 1000;
+  int dav_block = 0;
+  int hx_backend = 0;         // 0 auto, 1 CUDA cores, 2 tensor cores (tcgen05)
+  long long hx_calls = 0;     // K.X launches of the last solve
+  double hx_ms = 0;           // their summed device time
+  int hx_last_path = -1;      // 1 CUDA cores, 2 tcgen05
+  int num_sms = 148;
+  int dav_iters = 0;
+  double dav_maxres = 0;
+  DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo;
+};
+
+// status helpers
+xatu_status xatu_fail(xatu_ctx* ctx, xatu_status code, const std::string& msg);
+xatu_status xatu_cuda_fail(xatu_ctx* ctx, cudaError_t e, const char* where);
+
+// launchers implemented in the .cu files
+struct AsmParams;
+struct AsmInputs;
+struct AsmOutputs;
+
+// Davidson (davidson.cu): lowest nstates of H = diag + K (mixed) or H (FP64).
+xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec);
+// Dense FP64 (dense.cu): all eigenpairs with cuSOLVER.
+xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec);
+
+// K.X products (hx.cu).  Y[N x b] = (Khi + Klo) X, all row-major complex float.
+cudaError_t xatu_launch_hx_cuda_core(const __nv_bfloat162* Khi, const __nv_bfloat162* Klo, long long ldk, const float2* X,
+                                     float2* Y, long long N, int b, cudaStream_t s);
+// tcgen05 version (hx_tc.cu): Bt operands (ng x ldb bf16, hi/lo), Y column-major N x ng FP32.
+cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, long long ldk, const void* Bhi,
+                              const void* Blo, long long ldb, int ng, float* Y, int* status, int num_sms,
+                              cudaStream_t s);
+size_t xatu_hx_tc_smem(int ng);
+// W[:, col0 : col0 + nv] = H V[:, col0 : col0 + nv] with the current build (davidson.cu).
+xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv);
+
+#define XATU_CK(call)                                              \
+  do {                                                             \
+    cudaError_t e__ = (call);                                      \
+    if (e__ != cudaSuccess) return xatu_cuda_fail(ctx, e__, #call); \
+  } while (0)

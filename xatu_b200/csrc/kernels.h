@@ -1,0 +1,17 @@
+// Declarations of the engine's kernels and launchers (internal).
+#pragma once
+#include "params.h"
+
+extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int na, const double* motif, int ncells,
+                                                 const double* cells, int npairs, const int2* pairs, double* vtab);
+extern "C" __global__ void motif_ft_kernel(int nq, const double* q, int ncells, const double* cells, int npairs,
+                                           const int2* pairs, const double* vtab, double inv_total, int na, cd* out);
+extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nentries, const double* G, int na,
+                                              const double* motif, cd* W);
+extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na, const int* orb_off,
+                                                   const cd* eigvec, const cd* eigvecQ, const cd* VX, cd* L, cd* R);
+extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoints, const double* cellsR, const cd* HR,
+                                             double* eigval, cd* eigvec, int* status);
+extern "C" size_t band_solve_smem_per_warp(int norb, int nR);
+cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
+                                 bool force_generic, cudaStream_t s, int* path);

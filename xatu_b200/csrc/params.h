@@ -1,0 +1,64 @@
+// Launch-parameter structs shared by the host orchestration (api.cu) and
+// the kernels.  Passed by value as kernel arguments.
+#pragma once
+#include "common.cuh"
+
+// Reciprocal-space kernel table: entry e is the k - k' difference with
+// integer grid offsets (e / stride_d) % len_d - span_d along each reciprocal
+// axis, q = q0 + sum_d off_d b_d / n_eff.
+struct RecipTable {
+  int ndim;
+  int n_eff;
+  int span[3];
+  int len[3];
+  double b[9];            // reciprocal vectors (ndim x 3)
+  int nG;
+  double q0[3];
+};
+
+struct BandParams {
+  int nk;
+  int norb;
+  int nR;
+  int triangular;
+  int nb;                 // selected bands
+  int band_list[2 * XATU_MAX_BANDS];
+  double shift[3];        // k -> k + shift (Q)
+  int max_sweeps;
+};
+
+struct AsmParams {
+  int nk, nv, nc, nb, norb, na;
+  int64_t N;
+  int mode;          // 0 real space, 1 reciprocal space
+  int exchange;
+  double scissor;
+  EquivMap emap;
+  int rt_ndim;
+  int rt_len[3];
+  int rt_span[3];
+  int orb_off[XATU_MAX_ATOMS + 1];
+  int64_t nentries;  // rows of the interaction table
+  int64_t ldk;       // row pitch (complex elements) of the mixed-precision planes
+};
+
+struct AsmInputs {
+  const double* kpoints;   // nk x 3
+  const int* kgrid;        // nk x 3 integer grid offsets (reciprocal mode)
+  const double* eigval;    // nk x nb
+  const double* eigvalQ;
+  const cd* eigvec;        // nk x nb x norb
+  const cd* eigvecQ;
+  const cd* table;         // entries x na x na
+  const cd* exL;           // N x na
+  const cd* exR;           // N x na
+  int* status;             // device error word
+};
+
+struct AsmOutputs {
+  cd* H;                   // FP64: N x N
+  __nv_bfloat162* Khi;     // MIXED: N x N
+  __nv_bfloat162* Klo;
+  double* diag;            // MIXED: N
+};
+
