@@ -118,7 +118,7 @@ dav_small_eigh_kernel(const cd* __restrict__ T, int ld, int m, double* __restric
     A[r * lda + c] = T[r + (long long)c * ld];
   }
   __syncthreads();
-  const int sweeps = jacobi_eigh(g, A, lda, Vscratch, m, m, rot, scratch, max_sweeps, 1e-15);
+  const int sweeps = jacobi_eigh(g, A, lda, Vscratch, m, m, rot, scratch, max_sweeps, 1e-14);
   if (sweeps > max_sweeps && threadIdx.x == 0) atomicOr(status, XATU_DEVERR_NOCONV);
   jacobi_sort(g, A, lda, m, perm);
   for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
@@ -420,8 +420,6 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   const size_t vbytes = (size_t)N * mmax * sizeof(cd);
   XATU_CK(ctx->dv_V.ensure(vbytes));
   XATU_CK(ctx->dv_W.ensure(vbytes));
-  XATU_CK(ctx->dv_U.ensure((size_t)N * bsz * sizeof(cd)));
-  XATU_CK(ctx->dv_Y.ensure((size_t)N * bsz * sizeof(cd)));   // WU
   XATU_CK(ctx->dv_R.ensure((size_t)N * bsz * sizeof(cd)));
   XATU_CK(ctx->dv_tmp.ensure((size_t)N * mmax * sizeof(cd)));
   XATU_CK(ctx->dv_T.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd) * 2 + 4096));
@@ -430,8 +428,6 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   XATU_CK(ctx->dv_norm.ensure(4096 * sizeof(double)));
   cd* V = ctx->dv_V.as<cd>();
   cd* W = ctx->dv_W.as<cd>();
-  cd* U = ctx->dv_U.as<cd>();
-  cd* WU = ctx->dv_Y.as<cd>();
   cd* R = ctx->dv_R.as<cd>();
   const int ldT = DAV_MAX_BASIS;
   cd* T = ctx->dv_T.as<cd>();
@@ -474,7 +470,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
                                (DAV_MAX_BASIS + 1) * sizeof(int);
   XATU_CK(cudaFuncSetAttribute(dav_small_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigh_smem_max));
 
-  int m = 0, nnew = bsz;
+  // The basis V (and W = H V) is kept in Ritz form: after every Rayleigh-Ritz
+  // step V <- V Y, W <- W Y and T <- diag(theta), so the projected matrix of
+  // the next step is diagonal except for the rows and columns of the new
+  // corrections, and its Jacobi solve converges in a few sweeps.  A restart is
+  // a truncation to the lowest `bsz` Ritz vectors.
+  int m0 = 0, m = bsz;
   int it = 0;
   bool converged = false;
   std::vector<double> h_theta(ldT), h_norm(bsz);
@@ -484,12 +485,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   ctx->dav_maxres = 0;
   ctx->hx_calls = 0;
   ctx->hx_ms = 0;
+  cd* tmp = ctx->dv_tmp.as<cd>();
   for (it = 0; it < ctx->dav_max_iter; it++) {
-    // 1. W for the new block
-    XATU_TRY(xatu_apply_h(ctx, N, m, nnew));
-    const int m0 = m;
-    m += nnew;
-    // 2. new columns of T = V^H W
+    const int nnew = m - m0;
+    // 1. W for the new columns
+    XATU_TRY(xatu_apply_h(ctx, N, m0, nnew));
+    // 2. new columns of T = V^H W; the old block is already diag(theta)
     XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nnew, (int)N, &kOne, V, (int)N, W + (long long)m0 * N, (int)N,
                    &kZero, T + (long long)m0 * ldT, ldT));
     {
@@ -507,12 +508,17 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK(cudaGetLastError());
     }
+    // 4. rotate the basis into Ritz form (FP64 ZGEMMs through scratch)
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, m, m, &kOne, V, (int)N, Yr, ldT, &kZero, tmp, (int)N));
+    XATU_CK(cudaMemcpyAsync(V, tmp, sizeof(cd) * (size_t)N * m, cudaMemcpyDeviceToDevice, ctx->stream));
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, m, m, &kOne, W, (int)N, Yr, ldT, &kZero, tmp, (int)N));
+    XATU_CK(cudaMemcpyAsync(W, tmp, sizeof(cd) * (size_t)N * m, cudaMemcpyDeviceToDevice, ctx->stream));
+    dav_set_diag_kernel<<<(m * m + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, theta);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
     const int nritz = std::min(bsz, m);
-    // 4. Ritz vectors and their images
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, V, (int)N, Yr, ldT, &kZero, U, (int)N));
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, W, (int)N, Yr, ldT, &kZero, WU, (int)N));
-    // 5. residuals
-    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(U, WU, theta, N, R, norms);
+    // 5. residuals of the lowest Ritz pairs
+    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(V, W, theta, N, R, norms);
     ctx->launches++;
     XATU_CK(cudaGetLastError());
     XATU_CK(cudaMemcpyAsync(h_theta.data(), theta, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -522,7 +528,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(cudaStreamSynchronize(ctx->stream));
     if (st) {
       cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream);
-      return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz Jacobi did not converge");
+      return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz or K.X stage reported an error");
     }
     double maxres = 0;
     for (int s = 0; s < nstates; s++) maxres = std::max(maxres, h_norm[s]);
@@ -537,18 +543,13 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     }
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     if (el > wall_cap_s) break;
-    // 6. correction targets: unconverged among the kept Ritz pairs
+    // 6. correction targets: unconverged among the lowest Ritz pairs
     std::vector<int> sel;
     for (int s = 0; s < nritz; s++)
       if (h_norm[s] >= tol) sel.push_back(s);
     int nsel = (int)sel.size();
-    // 7. thick restart
+    // 7. restart = truncation (the basis is already in Ritz order)
     if (m + nsel > mmax) {
-      XATU_CK(cudaMemcpyAsync(V, U, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
-      XATU_CK(cudaMemcpyAsync(W, WU, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
-      dav_set_diag_kernel<<<(nritz * nritz + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, nritz, theta);
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
       m = nritz;
       if (m + nsel > mmax) nsel = mmax - m;
     }
@@ -564,12 +565,13 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     int kept = 0;
     XATU_TRY(orthonormalize_block(ctx, N, m, nsel, &kept));
     if (kept == 0) break;
-    nnew = kept;
+    m0 = m;
+    m += kept;
   }
-  // results
+  // results: the basis is in Ritz order, its first columns are the eigenvectors
   std::copy(h_theta.begin(), h_theta.begin() + nstates, eigval);
   if (eigvec)
-    XATU_CK(cudaMemcpyAsync(eigvec, U, sizeof(cd) * (size_t)N * nstates, cudaMemcpyDeviceToHost, ctx->stream));
+    XATU_CK(cudaMemcpyAsync(eigvec, V, sizeof(cd) * (size_t)N * nstates, cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   if (!converged) {
     char buf[160];
