@@ -22,8 +22,9 @@ def model_config(name):
 
 def oracle_system(cfg):
     si = cfg.systemInfo
+    ovl = si.overlap if getattr(si, "overlap", None) is not None and si.overlap.size else None
     return OracleSystem(si.ndim, si.bravaisLattice, si.motif, si.norbitals, si.bravaisVectors, si.hamiltonian,
-                        int(si.filling))
+                        int(si.filling), overlap=ovl)
 
 
 def oracle_exciton(cfg, ncell, nbands, params, Q=(0, 0, 0), mode="realspace", nG=1, exchange=False, factor=None,

@@ -152,6 +152,19 @@ def test_synthetic_22_orbital_small():
     assert np.abs(res.eigval - w).max() < ENERGY_TOL
 
 
+def test_loewdin_overlap_bands_and_matrix():
+    """Non-orthogonal basis: S(k)^-1/2 H(k) S(k)^-1/2 on the device (SystemTB.cpp:113-156)."""
+    from xatu_b200.synthetic import synthetic_hexagonal
+    cfg = synthetic_hexagonal(seed=77, orbitals=(4, 3, 3), overlap=0.08)
+    ex, orc = _pair(cfg, 8, 2, [1, 4.5, 40])
+    ev, vv, _, _ = ex.bandStacks()
+    assert np.abs(ev - orc.eigval).max() < 1e-10
+    # eigenvectors unique after the phase fix (random model: no degeneracies)
+    assert np.abs(vv - orc.eigvec).max() < 1e-8
+    ex.BShamiltonian("fp64")
+    assert rel_err(ex.HBS, orc.bs_hamiltonian()) < FP64_TOL
+
+
 def test_error_paths():
     from xatu_b200 import _lib as L
     cfg = model_config("hBN.model")

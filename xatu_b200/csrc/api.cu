@@ -33,7 +33,8 @@ static xatu_status check_device_status(xatu_ctx* ctx, const char* stage) {
   if (st & XATU_DEVERR_NAN) m += " non-finite input;";
   if (st & XATU_DEVERR_INDEX) m += " table index out of range;";
   if (st & XATU_DEVERR_NOCONV) m += " Jacobi sweep cap reached;";
-  return xatu_fail(ctx, (st & XATU_DEVERR_NAN) ? XATU_ERR_NUMERIC : XATU_ERR_NOT_CONVERGED, m);
+  if (st & XATU_DEVERR_OVERLAP) m += " Zero or negative overlap eigenvalues found;";
+  return xatu_fail(ctx, (st & (XATU_DEVERR_NAN | XATU_DEVERR_OVERLAP)) ? XATU_ERR_NUMERIC : XATU_ERR_NOT_CONVERGED, m);
 }
 
 template <typename T>
@@ -308,8 +309,6 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   if (!ctx) return XATU_ERR_INVALID;
   cudaSetDevice(ctx->device);
   if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
-  if (ctx->has_overlap)
-    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "non-orthogonal basis (overlap matrices) is not supported by this build");
   const size_t nk = ctx->nk, nb = ctx->nb, norb = ctx->norb;
   XATU_CK(ctx->d_eigval.ensure(nk * nb * sizeof(double)));
   XATU_CK(ctx->d_eigvec.ensure(nk * nb * norb * sizeof(cd)));
@@ -324,14 +323,17 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   bp.nb = ctx->nb;
   for (int i = 0; i < ctx->nb; i++) bp.band_list[i] = ctx->band_list[i];
   bp.max_sweeps = 40;
-  const size_t per_warp = band_solve_smem_per_warp(ctx->norb, ctx->nR);
+  bp.has_overlap = ctx->has_overlap ? 1 : 0;
+  bp.is_au = ctx->is_au ? 1 : 0;
+  const size_t per_warp = band_solve_smem_per_warp(ctx->norb, ctx->nR, bp.has_overlap);
   int warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / per_warp));
   const size_t smem = per_warp * warps;
   XATU_CK(cudaFuncSetAttribute(band_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int grid = (ctx->nk + warps - 1) / warps;
   XATU_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+  const cd* SR = ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr;
   band_solve_kernel<<<grid, 32 * warps, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
-                                                             ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(),
+                                                             ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                              ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
                                                              ctx->d_status.as<int>());
   ctx->launches++;
@@ -339,7 +341,7 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   if (ctx->qnonzero) {
     for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
     band_solve_kernel<<<grid, 32 * warps, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
-                                                               ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(),
+                                                               ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                                ctx->d_eigvalQ.as<double>(), ctx->d_eigvecQ.as<cd>(),
                                                                ctx->d_status.as<int>());
     ctx->launches++;

@@ -161,4 +161,4 @@ __device__ __forceinline__ int equivalent_index(const EquivMap& m, double dx, do
 // ----------------------------------------------------------------- error flag
 // Kernels never trap: out-of-contract indices are recorded in a device word the
 // host reads after the stage.
-enum { XATU_DEVERR_NONE = 0, XATU_DEVERR_INDEX = 1, XATU_DEVERR_NAN = 2, XATU_DEVERR_NOCONV = 4 };
+enum { XATU_DEVERR_NONE = 0, XATU_DEVERR_INDEX = 1, XATU_DEVERR_NAN = 2, XATU_DEVERR_NOCONV = 4, XATU_DEVERR_OVERLAP = 8 };

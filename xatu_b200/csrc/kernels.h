@@ -11,7 +11,7 @@ extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nen
 extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na, const int* orb_off,
                                                    const cd* eigvec, const cd* eigvecQ, const cd* VX, cd* L, cd* R);
 extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoints, const double* cellsR, const cd* HR,
-                                             double* eigval, cd* eigvec, int* status);
-extern "C" size_t band_solve_smem_per_warp(int norb, int nR);
+                                             const cd* SR, double* eigval, cd* eigvec, int* status);
+extern "C" size_t band_solve_smem_per_warp(int norb, int nR, int has_overlap);
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path);

@@ -25,6 +25,8 @@ struct BandParams {
   int band_list[2 * XATU_MAX_BANDS];
   double shift[3];        // k -> k + shift (Q)
   int max_sweeps;
+  int has_overlap;        // Loewdin orthogonalisation with S(k) (SystemTB.cpp:113-156)
+  int is_au;              // H in Hartree: scaled by 27.2 before the orthogonalisation (SystemTB.cpp:117-120)
 };
 
 struct AsmParams {

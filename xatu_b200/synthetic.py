@@ -48,7 +48,10 @@ def _herm_random(rng, n, sigma):
 
 
 def synthetic_hexagonal(seed: int = 1234, orbitals=(8, 7, 7), a: float = 3.0, sigma: float = 0.5,
-                        onsite: float = 2.0, shells: int = 2, filling: int | None = None) -> SyntheticConfiguration:
+                        onsite: float = 2.0, shells: int = 2, filling: int | None = None,
+                        overlap: float = 0.0) -> SyntheticConfiguration:
+    """``overlap`` > 0 adds non-orthogonal-basis overlap matrices S(R): identity plus
+    Hermitian random terms of that size on R = 0 and on the neighbour cells."""
     rng = np.random.default_rng(seed)
     a1 = np.array([a, 0.0, 0.0])
     a2 = np.array([a / 2, a * math.sqrt(3) / 2, 0.0])
@@ -69,6 +72,15 @@ def synthetic_hexagonal(seed: int = 1234, orbitals=(8, 7, 7), a: float = 3.0, si
         H[1 + p] = hr
         H[1 + npos + p] = hr.conj().T
     info = SystemInfo()
+    if overlap > 0:
+        S = np.zeros_like(H)
+        s0 = _herm_random(rng, norb, overlap)
+        S[0] = np.eye(norb) + 0.5 * (s0 + s0.conj().T)
+        for p in range(npos):
+            sr = _herm_random(rng, norb, overlap * 0.5)
+            S[1 + p] = sr
+            S[1 + npos + p] = sr.conj().T
+        info.overlap = S
     info.ndim = 2
     info.filling = float(filling if filling is not None else norb // 2)
     info.bravaisLattice = np.array([a1, a2])
