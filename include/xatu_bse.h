@@ -180,6 +180,22 @@ xatu_status xatu_kernel_stats(const xatu_ctx *ctx, int which, int64_t *launches,
 /* Number of engine kernels launched on this context since creation. */
 xatu_status xatu_kernel_launches(const xatu_ctx *ctx, int64_t *count);
 
+/* ------------------------------------------------------------------ allocation-free product */
+/* y = H x for a mixed build (FP64 diagonal + split-BF16 kernel planes), without any device allocation.
+   No counterpart in the reference: it exists for callers that cannot call cudaMalloc -- codes that keep
+   (nearly) all of the GPU's memory in their own pool, and caller-written iterative eigensolvers that request
+   the product thousands of times and cannot afford a cudaMalloc/cudaFree (device-wide synchronisation) per
+   request.  All arguments are device pointers owned by the caller: k_hi, k_lo, diag as returned by
+   xatu_bse_device_buffers for XATU_PREC_MIXED (n x ldk complex bf16 planes, ldk a multiple of 4), x and y
+   n x nvec complex128, column-major, 16-byte aligned.  Limits: n <= 16384, nvec <= 16; larger sizes return
+   XATU_ERR_UNSUPPORTED with a message on stderr.  Scratch is one static 6 MB device array per GPU that loads
+   the library, held until the process exits; the first call on a device looks up its address (do that first
+   call before any stream capture).  Every call shares that array and leaves its contents behind, so calls
+   that overlap on the GPU (other streams, other host threads) race.  Runs on `stream` (cudaStream_t, NULL =
+   legacy default stream) and waits for it before returning. */
+xatu_status xatu_hx_noalloc(const void *k_hi, const void *k_lo, const double *diag, int64_t n, int64_t ldk, int nvec,
+                            const double *x, double *y, void *stream);
+
 /* ------------------------------------------------------------------ geometry helpers (host, no device work) */
 /* Lattice::calculateReciprocalLattice (Lattice.cpp:56-80): out ndim x 3. */
 xatu_status xatu_reciprocal_lattice(int ndim, const double *bravais, double *recip);
