@@ -145,6 +145,11 @@ xatu_status xatu_motif_ft_download(xatu_ctx *ctx, double *ft_stack, double *ft_Q
 /* ------------------------------------------------------------------ BShamiltonian (ExcitonTB.cpp:840-921) */
 /* Runs the band solve and interaction tables if they are not current, then assembles H on the device. */
 xatu_status xatu_bse_build(xatu_ctx *ctx, int precision);
+/* ExcitonTB::BShamiltonian(const arma::imat& basis) (ExcitonTB.cpp:840-849): assemble H over a caller-given
+   subset of e-h states; basis: nbasis rows {valence band, conduction band, k index} with absolute band numbers
+   (the reference's basisStates layout).  The following solve works on this nbasis x nbasis matrix; a plain
+   xatu_bse_build returns to the full basis. */
+xatu_status xatu_bse_build_basis(xatu_ctx *ctx, int precision, int64_t nbasis, const int *basis);
 xatu_status xatu_bse_dim(const xatu_ctx *ctx, int64_t *n);
 /* Full Hermitian H, row-major N x N complex (FP64 build), or the mixed build expanded to complex128
    (diagonal band term + split-BF16 kernel). */
@@ -169,6 +174,14 @@ xatu_status xatu_hx_backend(xatu_ctx *ctx, int backend);
 /* Y = H X for nvec host vectors with the current build (X, Y: N x nvec complex, column-major); the product the
    Davidson iterations use. */
 xatu_status xatu_kernel_matvec(xatu_ctx *ctx, int nvec, const double *X, double *Y);
+
+/* ------------------------------------------------------------------ oscillator strengths */
+/* ResultTB::excitonOscillatorStrength (ResultTB.cpp:242-298; skubo_w.f90:175-330, 445-628): velocity matrix
+   elements of the excitons given by `eigvec` (host, N x nstates complex, column-major), in atomic units.
+   vme_ex receives 3 x nstates complex, column-major (the reference's 3 x N matrix restricted to these states).
+   Uses the band stacks of the context (bands computed or uploaded).  Unlike the reference, no argument is
+   modified in place. */
+xatu_status xatu_oscillator_strength(xatu_ctx *ctx, int nstates, const double *eigvec, double *vme_ex);
 
 /* ------------------------------------------------------------------ instrumentation */
 /* Device milliseconds of the last run of each stage: [0] bands, [1] interaction tables, [2] assembly,

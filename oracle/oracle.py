@@ -503,3 +503,88 @@ def array2hash(array, subview: bool = False) -> float:
     h = (np.abs(base).sum() + (base != 0).sum() + (np.real(cp) * 1.5).sum() + (np.imag(cp) * 1.5).sum()
          + (np.imag(cp) * np.real(cp)).sum()) / a.size
     return float(h)
+
+
+# ----------------------------------------------------------------------------- oscillator strengths
+
+BOHR = 0.52917721067121
+HARTREE = 27.211385
+
+
+def vme_single_particle(system: OracleSystem, k_au: np.ndarray, C: np.ndarray, e_au: np.ndarray) -> np.ndarray:
+    """Velocity matrix elements between the stored bands at one k (atomic units).
+
+    Restates get_vme_kernels + get_eigen_vme (skubo_w.f90:445-628) with the
+    hopping derivatives of hoppings_observables_TB (skubo_w.f90:407-443):
+    only the lower triangle (a' <= a) of every kernel is summed over R (with
+    R_z = 0), the upper triangle is filled by conjugation -- for the A kernel
+    as conj(A_aa') + i conj(S'_aa'), which also overwrites its diagonal -- and
+    the orbital positions enter through R index 0 only.  C: norb x nb band
+    coefficients, e_au: nb band energies (Hartree).  Returns vme[3][nb][nb]."""
+    norb = system.basisdim
+    R = system.cells_h / BOHR
+    H = system.hamiltonian / HARTREE                       # [R][a][a']
+    S = np.zeros_like(H)
+    if system.overlap is not None and len(system.overlap):
+        S = np.real(system.overlap).astype(np.complex128)
+    else:
+        S[:] = np.eye(norb)[None, :, :]
+    pos = np.zeros((norb, 3))
+    for a in range(system.natoms):
+        pos[system.orb_offset[a]:system.orb_offset[a + 1]] = system.motif[a, :3] / BOHR
+    nR = R.shape[0]
+    lower = np.tril(np.ones((norb, norb), dtype=bool))
+    phase = np.exp(1j * (k_au[0] * R[:, 0] + k_au[1] * R[:, 1] + k_au[2] * 0.0))   # R_z = 0
+    hk = np.einsum("r,rab->ab", phase, H)
+    sk = np.einsum("r,rab->ab", phase, S)
+    hder = np.zeros((3, norb, norb), dtype=np.complex128)
+    sder = np.zeros((3, norb, norb), dtype=np.complex128)
+    for nj, comp in ((0, R[:, 0]), (1, R[:, 1])):
+        hder[nj] = np.einsum("r,rab->ab", phase * 1j * comp, H)
+        sder[nj] = np.einsum("r,rab->ab", phase * 1j * comp, S)
+    akern = np.zeros((3, norb, norb), dtype=np.complex128)
+    for nj in range(3):
+        # rhop(nj, R index 0, a, a) = position of orbital a
+        akern[nj] = 1j * sder[nj] + np.diag(pos[:, nj]) * phase[0]
+    # lower triangle kept, upper from conjugation
+    hk_f = np.where(lower, hk, hk.T.conj())
+    hder_f = np.where(lower[None], hder, np.transpose(hder, (0, 2, 1)).conj())
+    for nj in range(3):
+        np.fill_diagonal(hder_f[nj], np.diag(hder[nj]).conj())   # the mirror loop also conjugates the diagonal
+    sder_l = np.where(lower[None], sder, 0)
+    ak_f = np.where(lower[None], akern, np.transpose(akern, (0, 2, 1)).conj()
+                    + 1j * np.transpose(sder_l, (0, 2, 1)).conj())
+    # diagonal: overwritten by conj(A_aa) + i conj(S'_aa)
+    for nj in range(3):
+        d = np.diag(akern[nj]).conj() + 1j * np.diag(sder[nj]).conj()
+        np.fill_diagonal(ak_f[nj], d)
+    nb = C.shape[1]
+    vme = np.zeros((3, nb, nb), dtype=np.complex128)
+    for nn in range(nb):
+        for nnp in range(nn + 1):
+            cc = np.outer(C[:, nn].conj(), C[:, nnp])               # conj(amu) * amup  [a][a']
+            for nj in range(3):
+                va = np.sum(cc * hder_f[nj])
+                vb = np.sum(cc * (e_au[nn] * ak_f[nj] - e_au[nnp] * ak_f[nj].T.conj())) * 1j
+                vme[nj, nn, nnp] = va + vb
+                vme[nj, nnp, nn] = np.conj(va + vb)
+    return vme
+
+
+def exciton_oscillator_strength(ex: "OracleExciton", eigvec: np.ndarray) -> np.ndarray:
+    """ResultTB::excitonOscillatorStrength (ResultTB.cpp:242-298) with
+    exciton_oscillator_strength (skubo_w.f90:175-330): returns vme_ex[3][nstates],
+    vme_ex(nj, s) = sum_j X(j, s) vme(k_j, nj, v_j, c_j) (no conjugation of X).
+    Unlike the reference, the exciton energies are not converted in place."""
+    s = ex.system
+    nv, nc = len(ex.valence), len(ex.conduction)
+    nk = ex.kpoints.shape[0]
+    v = np.zeros((3, ex.N), dtype=np.complex128)
+    for ik in range(nk):
+        C = ex.eigvec[ik].T                                         # norb x nb
+        vme = vme_single_particle(s, ex.kpoints[ik] * BOHR, C, ex.eigval[ik] / HARTREE)
+        for ic in range(nc):
+            for iv in range(nv):
+                j = ik * nc * nv + ic * nv + iv
+                v[:, j] = vme[:, iv, nv + ic]
+    return v @ eigvec

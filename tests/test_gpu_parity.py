@@ -165,6 +165,51 @@ def test_loewdin_overlap_bands_and_matrix():
     assert rel_err(ex.HBS, orc.bs_hamiltonian()) < FP64_TOL
 
 
+@pytest.mark.parametrize("model,ncell,nbands,params,golden", [
+    ("hBN.model", 20, 1, [1, 1, 10], 47.4140063784),          # tests.cpp:371-399
+    ("MoS2.model", 12, 2, [1., 4., 13.55], 37.2792093358),    # tests.cpp:776-804
+])
+def test_oscillator_strength_golden_and_oracle(model, ncell, nbands, params, golden):
+    """Device band solve + dense solve + oscillator strengths against the reference golden
+    (sum over all excitons) and against the oracle for the lowest states."""
+    from oracle.oracle import exciton_oscillator_strength
+    cfg = model_config(model)
+    ex, orc = _pair(cfg, ncell, nbands, params)
+    ex.BShamiltonian("fp64")
+    N = ex.excitonbasisdim
+    res = ex.diagonalize("diag", N)
+    vx = ex.excitonOscillatorStrength(res.eigvec)
+    assert float(np.sum(np.abs(vx) ** 2)) == pytest.approx(golden, abs=1e-7)
+    # same bands on both sides: per-state agreement for the lowest states
+    ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
+    X = np.linalg.eigh(orc.bs_hamiltonian())[1][:, :6]
+    v_dev = ex.excitonOscillatorStrength(X)
+    v_orc = exciton_oscillator_strength(orc, X)
+    assert np.abs(v_dev - v_orc).max() < 1e-9 * max(1.0, np.abs(v_orc).max())
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_caller_given_basis(precision, tol):
+    """BShamiltonian(const arma::imat& basis): a shuffled subset of the e-h states, with exchange and Q."""
+    cfg = model_config("MoS2.model")
+    kw = dict(Q=(0, 0.05, 0), exchange=True)
+    ex, orc = _pair(cfg, 6, 2, [1., 4., 13.55], **kw)
+    ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
+    Ho = orc.bs_hamiltonian()
+    rng = np.random.default_rng(4)
+    idx = rng.permutation(orc.N)[:90]
+    fl = orc.system.fermi_level
+    rows = np.stack([orc.valence[orc.basis_v[idx]], orc.conduction[orc.basis_c[idx] - len(orc.valence)],
+                     orc.basis_k[idx]], axis=1)
+    ex.BShamiltonianBasis(rows, precision)
+    H = ex.HBS
+    assert H.shape == (90, 90)
+    assert rel_err(H, Ho[np.ix_(idx, idx)]) < tol
+    # back to the full basis
+    ex.BShamiltonian(precision)
+    assert ex.HBS.shape == Ho.shape
+
+
 def test_error_paths():
     from xatu_b200 import _lib as L
     cfg = model_config("hBN.model")

@@ -46,6 +46,19 @@ def test_oracle_kwf_hash(key):
     assert array2hash(kwf) == pytest.approx(g["hash"], abs=g["tol"])
 
 
+@pytest.mark.parametrize("model,ncell,nbands,params,golden", [
+    ("hBN.model", 20, 1, [1, 1, 10], 47.4140063784),          # tests.cpp:371-399
+    ("MoS2.model", 12, 2, [1., 4., 13.55], 37.2792093358),    # tests.cpp:776-804
+])
+def test_oracle_oscillator_strength_sum(model, ncell, nbands, params, golden):
+    from oracle.oracle import exciton_oscillator_strength
+    ex = oracle_exciton(model_config(model), ncell, nbands, params)
+    ex.bs_hamiltonian()
+    w, v = ex.diagonalize("diag")
+    vx = exciton_oscillator_strength(ex, v)
+    assert float(np.sum(np.abs(vx) ** 2)) == pytest.approx(golden, abs=1e-7)
+
+
 def test_oracle_matrix_is_hermitian_and_diag_real():
     cfg = model_config("MoS2.model")
     ex = oracle_exciton(cfg, 6, 2, [1., 4., 13.55], Q=(0, 0.1, 0), exchange=True)

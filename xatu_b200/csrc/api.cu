@@ -78,7 +78,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
   if (!ctx) return XATU_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  DBuf* bufs[] = {&ctx->d_motif, &ctx->d_orboff, &ctx->d_cellsR, &ctx->d_HR, &ctx->d_SR, &ctx->d_kpoints, &ctx->d_mesh,
+  DBuf* bufs[] = {&ctx->d_motif, &ctx->d_orboff, &ctx->d_basis, &ctx->d_cellsR, &ctx->d_HR, &ctx->d_SR, &ctx->d_kpoints, &ctx->d_mesh,
                   &ctx->d_cells, &ctx->d_G, &ctx->d_kgrid, &ctx->d_eigval, &ctx->d_eigvec, &ctx->d_eigvalQ,
                   &ctx->d_eigvecQ, &ctx->d_pairs, &ctx->d_vtab, &ctx->d_vtabX, &ctx->d_table, &ctx->d_VX,
                   &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status,
@@ -229,6 +229,8 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
   ctx->nc = e->nconduction;
   ctx->nb = ctx->nv + ctx->nc;
   ctx->N = (long long)e->nk * ctx->nv * ctx->nc;
+  ctx->N_full = ctx->N;
+  ctx->custom_basis = false;
   ctx->ldk = (ctx->N + 3) / 4 * 4;
   ctx->band_list = bl;
   ctx->eps_m = e->eps_m;
@@ -517,9 +519,45 @@ xatu_status xatu_motif_ft_download(xatu_ctx* ctx, double* ft_stack, double* ft_Q
 }
 
 // ------------------------------------------------------------------ assembly
+static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis);
+
 xatu_status xatu_bse_build(xatu_ctx* ctx, int precision) {
   if (!ctx) return XATU_ERR_INVALID;
   cudaSetDevice(ctx->device);
+  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+  ctx->N = ctx->N_full;
+  ctx->ldk = (ctx->N + 3) / 4 * 4;
+  ctx->custom_basis = false;
+  return build_impl(ctx, precision, nullptr);
+}
+
+xatu_status xatu_bse_build_basis(xatu_ctx* ctx, int precision, int64_t nbasis, const int* basis) {
+  if (!ctx || !basis || nbasis < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
+  cudaSetDevice(ctx->device);
+  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+  // absolute band numbers -> stack columns (Exciton::generateBandDictionary, Exciton.tpp:191-199)
+  std::vector<int> rows(3 * (size_t)nbasis);
+  for (int64_t i = 0; i < nbasis; i++) {
+    const int vb = basis[3 * i], cb = basis[3 * i + 1], k = basis[3 * i + 2];
+    int vcol = -1, crel = -1;
+    for (int b = 0; b < ctx->nv; b++)
+      if (ctx->band_list[b] == vb) vcol = b;
+    for (int b = 0; b < ctx->nc; b++)
+      if (ctx->band_list[ctx->nv + b] == cb) crel = b;
+    if (vcol < 0 || crel < 0 || k < 0 || k >= ctx->nk)
+      return xatu_fail(ctx, XATU_ERR_INVALID, "basis row outside the exciton's bands or k points");
+    rows[3 * i] = k;
+    rows[3 * i + 1] = vcol;
+    rows[3 * i + 2] = crel;
+  }
+  XATU_CK(upload(ctx->d_basis, rows.data(), rows.size(), ctx->stream));
+  ctx->N = nbasis;
+  ctx->ldk = (ctx->N + 3) / 4 * 4;
+  ctx->custom_basis = true;
+  return build_impl(ctx, precision, ctx->d_basis.as<int>());
+}
+
+static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis) {
   if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
   if (precision != XATU_PREC_FP64 && precision != XATU_PREC_MIXED)
     return xatu_fail(ctx, XATU_ERR_INVALID, "precision must be XATU_PREC_FP64 or XATU_PREC_MIXED");
@@ -575,6 +613,7 @@ xatu_status xatu_bse_build(xatu_ctx* ctx, int precision) {
   in.exL = ctx->d_exL.as<cd>();
   in.exR = ctx->d_exR.as<cd>();
   in.status = ctx->d_status.as<int>();
+  in.basis = basis;
   AsmOutputs out;
   out.H = ctx->d_H.as<cd>();
   out.Khi = ctx->d_Khi.as<__nv_bfloat162>();
@@ -585,14 +624,14 @@ xatu_status xatu_bse_build(xatu_ctx* ctx, int precision) {
     const int blocks = (int)((N + 127) / 128);
     exchange_vectors_kernel<<<blocks, 128, 0, ctx->stream>>>((int)N, ctx->nv, ctx->nc, ctx->nb, ctx->norb, na,
                                                              ctx->d_orboff.as<int>(), ctx->d_eigvec.as<cd>(),
-                                                             ctx->d_eigvecQ.as<cd>(), ctx->d_VX.as<cd>(),
+                                                             ctx->d_eigvecQ.as<cd>(), ctx->d_VX.as<cd>(), basis,
                                                              ctx->d_exL.as<cd>(), ctx->d_exR.as<cd>());
     ctx->launches++;
     XATU_CK(cudaGetLastError());
   }
   int path = -1;
   const char* force = getenv("XATU_FORCE_GENERIC_ASSEMBLY");
-  XATU_CK(xatu_launch_assembly(p, in, out, mixed, force && force[0] == '1', ctx->stream, &path));
+  XATU_CK(xatu_launch_assembly(p, in, out, mixed, (force && force[0] == '1') || basis != nullptr, ctx->stream, &path));
   ctx->launches++;
   ctx->last_assembly_path = path;
   XATU_CK(cudaEventRecord(ctx->ev[5], ctx->stream));

@@ -123,6 +123,27 @@ bse_assemble_tile_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
   E* sL = sTile + TR * LDT;                                // [TR][NA] exchange rows
   E* sR = sL + TR * NA;                                    // [TR][NA] exchange columns
   const int tid = threadIdx.x;
+  const int kk = tid / TK, kk2 = tid % TK;
+  const int k = kb * TK + kk, k2 = kb2 * TK + kk2;
+  const bool active = (k < p.nk) && (k2 < p.nk) && !(kb == kb2 && k > k2);
+  // FP32 path: the pair's interaction-table row goes to registers before the
+  // staging barrier, so its L2 latency overlaps the coefficient staging.
+  constexpr bool kPrefetchV = sizeof(T) == 4;
+  E Vr[kPrefetchV ? NA : 1][kPrefetchV ? NA : 1];
+  const cd* Vt = nullptr;
+  if (active) {
+    Vt = interaction_ptr(p, in, k, k2);
+    if (kPrefetchV) {
+#pragma unroll
+      for (int a = 0; a < (kPrefetchV ? NA : 1); a++)
+#pragma unroll
+        for (int b = 0; b < (kPrefetchV ? NA : 1); b++) {
+          const cd v = Vt[a * NA + b];
+          Vr[a][b] = {(T)v.x, (T)v.y};
+        }
+    }
+  }
+#pragma unroll 4
   for (int t = tid; t < 2 * side_sz; t += blockDim.x) {
     const int side = t / side_sz;
     const int r = t - side * side_sz;
@@ -161,14 +182,10 @@ bse_assemble_tile_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
     }
   }
   __syncthreads();
-  const int kk = tid / TK, kk2 = tid % TK;
-  const int k = kb * TK + kk, k2 = kb2 * TK + kk2;
-  const bool active = (k < p.nk) && (k2 < p.nk) && !(kb == kb2 && k > k2);
   if (active) {
     const E* C1 = sC;
     const E* C2 = sC + side_sz;
 #define SCO(S, band, o, q) (S)[((band) * norb + (o)) * TK + (q)]
-    const cd* Vt = interaction_ptr(p, in, k, k2);
     // T_a(v', v) = sum_b V_ab rho2_b(v', v)
     E Tm[NA][NV][NV];
 #pragma unroll
@@ -198,8 +215,13 @@ bse_assemble_tile_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
       }
 #pragma unroll
       for (int a = 0; a < NA; a++) {
-        const cd vab = Vt[a * NA + b];
-        const E V = {(T)vab.x, (T)vab.y};
+        E V;
+        if (kPrefetchV) {
+          V = Vr[kPrefetchV ? a : 0][kPrefetchV ? b : 0];
+        } else {
+          const cd vab = Vt[a * NA + b];
+          V = {(T)vab.x, (T)vab.y};
+        }
 #pragma unroll
         for (int v2 = 0; v2 < NV; v2++)
 #pragma unroll
@@ -357,10 +379,20 @@ __global__ void bse_assemble_generic_kernel(AsmParams p, AsmInputs in, AsmOutput
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   for (int64_t i = blockIdx.y; i < p.N; i += gridDim.y) {
   if (j >= p.N || j < i) continue;
-  const int ncv = p.nc * p.nv;
-  const int k = (int)(i / ncv), k2 = (int)(j / ncv);
-  const int c = (int)((i - (int64_t)k * ncv) / p.nv), v = (int)(i - (int64_t)k * ncv - c * p.nv);
-  const int c2 = (int)((j - (int64_t)k2 * ncv) / p.nv), v2 = (int)(j - (int64_t)k2 * ncv - c2 * p.nv);
+  int k, c, v, k2, c2, v2;
+  if (in.basis) {
+    // caller-given basis rows (ExcitonTB::BShamiltonian(const arma::imat&), ExcitonTB.cpp:840-849)
+    k = in.basis[3 * i]; v = in.basis[3 * i + 1]; c = in.basis[3 * i + 2];
+    k2 = in.basis[3 * j]; v2 = in.basis[3 * j + 1]; c2 = in.basis[3 * j + 2];
+  } else {
+    const int ncv = p.nc * p.nv;
+    k = (int)(i / ncv);
+    k2 = (int)(j / ncv);
+    c = (int)((i - (int64_t)k * ncv) / p.nv);
+    v = (int)(i - (int64_t)k * ncv - c * p.nv);
+    c2 = (int)((j - (int64_t)k2 * ncv) / p.nv);
+    v2 = (int)(j - (int64_t)k2 * ncv - c2 * p.nv);
+  }
   const cd* Vt = interaction_ptr(p, in, k, k2);
   const cd* Cc = in.eigvecQ + ((int64_t)k * p.nb + p.nv + c) * p.norb;
   const cd* Cc2 = in.eigvecQ + ((int64_t)k2 * p.nb + p.nv + c2) * p.norb;
@@ -396,7 +428,8 @@ static cudaError_t launch_tile(const AsmParams& p, const AsmInputs& in, const As
   const int nblk = (p.nk + ASM_TK - 1) / ASM_TK;
   const int ntiles = nblk * (nblk + 1) / 2;
   constexpr int TR = ASM_TK * NV * NC;
-  const size_t smem = (2 * (size_t)(NV + NC) * p.norb * ASM_TK + (size_t)TR * (TR + 1) + 2 * (size_t)TR * NA) *
+  const size_t smem = (2 * (size_t)(NV + NC) * p.norb * ASM_TK + (size_t)TR * (TR + 1) +
+                       (p.exchange ? 2 * (size_t)TR * NA : 0)) *
                       sizeof(cplx<T>);
   auto kern = bse_assemble_tile_kernel<T, NV, NC, NA, MIXED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -439,7 +472,7 @@ cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const 
   const int tr = ASM_TK * p.nv * p.nc;
   const size_t smem_f64 = (2 * (size_t)(p.nv + p.nc) * p.norb * ASM_TK + (size_t)tr * (tr + 1) + 2 * (size_t)tr * 4) *
                           sizeof(cd);
-  const bool pair_ok = !force_generic && smem_f64 <= 200 * 1024;
+  const bool pair_ok = !force_generic && in.basis == nullptr && smem_f64 <= 200 * 1024;
   cudaError_t e = cudaSuccess;
   bool launched = false;
   if (pair_ok) {

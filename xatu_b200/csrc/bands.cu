@@ -14,7 +14,8 @@
 #include "jacobi.cuh"
 #include "params.h"
 
-__device__ __forceinline__ int band_lda(int n) { return n + 1; }
+// Odd row pitch (in 16-byte elements) keeps the lane-per-row passes bank-conflict free.
+__host__ __device__ __forceinline__ int band_lda(int n) { return (n % 2 == 0) ? n + 1 : n + 2; }
 
 // Bloch sum of a [R][row][col] stack into M (row stride ld), with the
 // triangular-storage symmetrisation of SystemTB::hamiltonian (SystemTB.cpp:69-72);
@@ -99,7 +100,7 @@ extern "C" __global__ void band_solve_kernel(BandParams bp, const double* __rest
     // B = h (scaled), A = S(k); Jacobi of S into (A, V); A = X = V diag(l^-1/2) V^H; h' = X h X -> A
     bloch_sum(g, HR, ph, bp.nR, n, lda, bp.triangular, bp.is_au ? 27.2 : 1.0, B, V);
     bloch_sum(g, SR, ph, bp.nR, n, lda, bp.triangular, 1.0, A, V);
-    const int sw = jacobi_eigh(g, A, lda, V, lda, n, rot, nullptr, bp.max_sweeps, 1e-15);
+    const int sw = jacobi_eigh_warp(A, lda, V, lda, n, rot, bp.max_sweeps, 1e-15);
     if (sw > bp.max_sweeps && lane == 0) atomicOr(status, XATU_DEVERR_NOCONV);
     bool nonpos = false;
     for (int i = lane; i < n; i += 32) nonpos |= !(A[i * lda + i].x > 0.0);
@@ -140,7 +141,7 @@ extern "C" __global__ void band_solve_kernel(BandParams bp, const double* __rest
     if (lane == 0) atomicOr(status, XATU_DEVERR_NAN);
     return;
   }
-  const int sweeps = jacobi_eigh(g, A, lda, V, lda, n, rot, nullptr, bp.max_sweeps, 1e-15);
+  const int sweeps = jacobi_eigh_warp(A, lda, V, lda, n, rot, bp.max_sweeps, 1e-15);
   if (sweeps > bp.max_sweeps && lane == 0) atomicOr(status, XATU_DEVERR_NOCONV);
   jacobi_sort(g, A, lda, n, perm);
   for (int b = 0; b < bp.nb; b++) {
@@ -164,7 +165,7 @@ extern "C" __global__ void band_solve_kernel(BandParams bp, const double* __rest
 }
 
 extern "C" size_t band_solve_smem_per_warp(int norb, int nR, int has_overlap) {
-  const int n = norb, lda = n + 1;
+  const int n = norb, lda = band_lda(n);
   const size_t matsz = (size_t)n * lda;
   const size_t per_warp = (has_overlap ? 3 : 2) * matsz * sizeof(cd) + (size_t)(n / 2 + 2) * sizeof(JacobiRot) +
                           (size_t)nR * sizeof(cd) + (size_t)(n + 1) * sizeof(int);

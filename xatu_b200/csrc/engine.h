@@ -57,6 +57,8 @@ struct xatu_ctx {
   bool has_exciton = false;
   int ncell = 0, factor = 1, n_eff = 0, nk = 0, nmesh = 0, nv = 0, nc = 0, nb = 0;
   long long N = 0;
+  long long N_full = 0;        // nk * nv * nc
+  bool custom_basis = false;   // last build used a caller-given basis
   long long ldk = 0;          // row pitch of the mixed planes (N rounded up to 4)
   std::vector<int> band_list;
   double eps_m = 1, eps_s = 1, r0 = 1, regularization = 0, cutoff = 0, scissor = 0;
@@ -69,7 +71,7 @@ struct xatu_ctx {
   bool kgrid_ok = false;
   int rt_len[3] = {1, 1, 1}, rt_span[3] = {0, 0, 0};
   long long rt_entries = 1;
-  DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid;
+  DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid, d_basis;
 
   // ---------------- derived device data
   bool bands_ok = false, tables_ok = false;

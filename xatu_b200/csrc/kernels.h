@@ -9,7 +9,8 @@ extern "C" __global__ void motif_ft_kernel(int nq, const double* q, int ncells, 
 extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nentries, const double* G, int na,
                                               const double* motif, cd* W);
 extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na, const int* orb_off,
-                                                   const cd* eigvec, const cd* eigvecQ, const cd* VX, cd* L, cd* R);
+                                                   const cd* eigvec, const cd* eigvecQ, const cd* VX, const int* basis,
+                                                   cd* L, cd* R);
 extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoints, const double* cellsR, const cd* HR,
                                              const cd* SR, double* eigval, cd* eigvec, int* status);
 extern "C" size_t band_solve_smem_per_warp(int norb, int nR, int has_overlap);

@@ -141,13 +141,21 @@ extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nen
 extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na,
                                                    const int* __restrict__ orb_off, const cd* __restrict__ eigvec,
                                                    const cd* __restrict__ eigvecQ, const cd* __restrict__ VX,
-                                                   cd* __restrict__ L, cd* __restrict__ R) {
+                                                   const int* __restrict__ basis, cd* __restrict__ L,
+                                                   cd* __restrict__ R) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const int ncv = nc * nv;
-  const int k = i / ncv;
-  const int c = (i - k * ncv) / nv;
-  const int v = i - k * ncv - c * nv;
+  int k, c, v;
+  if (basis) {
+    k = basis[3 * i];
+    v = basis[3 * i + 1];
+    c = basis[3 * i + 2];
+  } else {
+    const int ncv = nc * nv;
+    k = i / ncv;
+    c = (i - k * ncv) / nv;
+    v = i - k * ncv - c * nv;
+  }
   const cd* cv = eigvec + ((int64_t)k * nb + v) * norb;
   const cd* cc = eigvecQ + ((int64_t)k * nb + nv + c) * norb;
   cd rho[XATU_MAX_ATOMS];

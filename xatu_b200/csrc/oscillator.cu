@@ -1,0 +1,182 @@
+// Exciton oscillator strengths (ResultTB::excitonOscillatorStrength,
+// ResultTB.cpp:242-298, with exciton_oscillator_strength / get_vme_kernels /
+// get_eigen_vme of skubo_w.f90:175-330, 445-628), in atomic units as the
+// reference returns them.
+//
+// vme_kernel: one CTA per k.  For each Cartesian direction it builds in shared
+// memory the Bloch kernels of the hopping derivative and of the position
+// ("A") operator -- summing only the lower triangle over R (R_z = 0) and filling
+// the upper triangle by conjugation, the A kernel as conj(A) + i conj(S'), which
+// also replaces its diagonal, exactly as the reference does -- and contracts
+// them with the stored band coefficients:
+//   vme(n, n') = sum_{a,a'} conj(C_a n) C_a' n' [ H'_aa' + i (e_n A_aa' - e_n' conj(A_a'a)) ]
+// for n = conduction, n' = valence; the element the exciton sum uses is
+// vme(v, c) = conj(vme(c, v)).
+// exciton_vme_kernel: vme_ex(j, s) = sum_i X_is v_j(i), one CTA per (j, s).
+#include "engine.h"
+
+#define OSC_BOHR 0.52917721067121
+#define OSC_HARTREE 27.211385
+
+struct OscParams {
+  int nk, norb, nR, nb, nv, nc, natoms;
+  int has_overlap;
+  int orb_off[XATU_MAX_ATOMS + 1];
+  double pos[3 * XATU_MAX_ATOMS];   // atom positions (Angstrom)
+};
+
+extern "C" __global__ void vme_kernel(OscParams p, const double* __restrict__ kpoints, const double* __restrict__ cellsR,
+                                      const cd* __restrict__ HR, const cd* __restrict__ SR,
+                                      const double* __restrict__ eigval, const cd* __restrict__ eigvec,
+                                      cd* __restrict__ vout /* 3 x N, row-major */) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = p.norb;
+  const int k = blockIdx.x;
+  cd* Hd = reinterpret_cast<cd*>(smem_raw);   // n x n
+  cd* Ak = Hd + n * n;                        // n x n
+  cd* ph = Ak + n * n;                        // nR
+  cd* C = ph + p.nR;                          // nb x n
+  double* e = reinterpret_cast<double*>(C + p.nb * n);   // nb
+  const double kx = kpoints[3 * k] * OSC_BOHR, ky = kpoints[3 * k + 1] * OSC_BOHR;
+  for (int r = threadIdx.x; r < p.nR; r += blockDim.x) {
+    double s, c;
+    sincos(kx * (cellsR[3 * r] / OSC_BOHR) + ky * (cellsR[3 * r + 1] / OSC_BOHR), &s, &c);
+    ph[r] = mk(c, s);
+  }
+  for (int t = threadIdx.x; t < p.nb * n; t += blockDim.x) C[t] = eigvec[(int64_t)k * p.nb * n + t];
+  for (int b = threadIdx.x; b < p.nb; b += blockDim.x) e[b] = eigval[(int64_t)k * p.nb + b] / OSC_HARTREE;
+  __syncthreads();
+  const int N = p.nk * p.nv * p.nc;
+  for (int nj = 0; nj < 3; nj++) {
+    // lower-triangle Bloch sums, then the conjugate fill of the upper triangle
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int a = t / n, a2 = t - a * n;
+      if (a2 > a) continue;
+      cd hd = mk(0, 0), sd = mk(0, 0);
+      if (nj < 2) {
+        for (int r = 0; r < p.nR; r++) {
+          const double Rc = cellsR[3 * r + nj] / OSC_BOHR;
+          const cd f = mk(-Rc * ph[r].y, Rc * ph[r].x);   // i R e^{ik.R}
+          hd = hd + f * ((1.0 / OSC_HARTREE) * HR[(int64_t)r * n * n + a * n + a2]);
+          const cd s = p.has_overlap ? mk(SR[(int64_t)r * n * n + a * n + a2].x, 0.0) : mk(a == a2 ? 1.0 : 0.0, 0.0);
+          sd = sd + f * s;
+        }
+      }
+      // A = sum_R e^{ikR} (r_hop + i S'_hop); r_hop holds the orbital position on R index 0 only
+      cd ak = mk(-sd.y, sd.x);
+      if (a == a2) {
+        int atom = 0;
+        while (atom + 1 < p.natoms && a >= p.orb_off[atom + 1]) atom++;
+        ak = ak + (p.pos[3 * atom + nj] / OSC_BOHR) * ph[0];
+      }
+      const cd isdc = mk(sd.y, sd.x);   // i conj(S')
+      if (a == a2) {
+        Hd[a * n + a] = conj(hd);
+        Ak[a * n + a] = conj(ak) + isdc;
+      } else {
+        Hd[a * n + a2] = hd;
+        Hd[a2 * n + a] = conj(hd);
+        Ak[a * n + a2] = ak;
+        Ak[a2 * n + a] = conj(ak) + isdc;
+      }
+    }
+    __syncthreads();
+    // one warp per (valence, conduction) pair
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int pr = warp; pr < p.nv * p.nc; pr += nw) {
+      const int ic = pr / p.nv, iv = pr - ic * p.nv;
+      const int nn = p.nv + ic, nnp = iv;
+      const double en = e[nn], enp = e[nnp];
+      cd acc = mk(0, 0);
+      for (int t = lane; t < n * n; t += 32) {
+        const int a = t / n, a2 = t - a * n;
+        const cd w = cmulc(C[nn * n + a], C[nnp * n + a2]);   // conj(C_a n) C_a' n'
+        const cd A1 = Ak[a * n + a2], A2c = conj(Ak[a2 * n + a]);
+        const cd bterm = mk(en * A1.x - enp * A2c.x, en * A1.y - enp * A2c.y);
+        const cd term = Hd[a * n + a2] + mk(-bterm.y, bterm.x);
+        acc = acc + w * term;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+      }
+      if (lane == 0) {
+        const int j = k * p.nc * p.nv + ic * p.nv + iv;
+        vout[(int64_t)nj * N + j] = conj(acc);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+extern "C" __global__ void exciton_vme_kernel(const cd* __restrict__ v, const cd* __restrict__ X, int N, int ns,
+                                              cd* __restrict__ out /* 3 x ns, column-major */) {
+  const int nj = blockIdx.x % 3, s = blockIdx.x / 3;
+  cd acc = mk(0, 0);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) acc = acc + X[(int64_t)s * N + i] * v[(int64_t)nj * N + i];
+  __shared__ double rr[32], ri[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    rr[threadIdx.x >> 5] = acc.x;
+    ri[threadIdx.x >> 5] = acc.y;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      a += rr[w];
+      b += ri[w];
+    }
+    out[(int64_t)s * 3 + nj] = mk(a, b);
+  }
+}
+
+extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, const double* eigvec, double* vme_ex) {
+  if (!ctx || !eigvec || !vme_ex || nstates < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
+  cudaSetDevice(ctx->device);
+  if (!ctx->bands_ok) return xatu_fail(ctx, XATU_ERR_STATE, "bands are not computed");
+  if (ctx->custom_basis)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "oscillator strengths need the full e-h basis (last build used a subset)");
+  if (nstates > ctx->N) return xatu_fail(ctx, XATU_ERR_INVALID, "nstates larger than the BSE dimension");
+  const long long N = ctx->N;
+  OscParams p;
+  memset(&p, 0, sizeof(p));
+  p.nk = ctx->nk;
+  p.norb = ctx->norb;
+  p.nR = ctx->nR;
+  p.nb = ctx->nb;
+  p.nv = ctx->nv;
+  p.nc = ctx->nc;
+  p.natoms = ctx->natoms;
+  p.has_overlap = ctx->has_overlap ? 1 : 0;
+  for (int a = 0; a <= ctx->natoms; a++) p.orb_off[a] = ctx->orb_off[a];
+  for (int a = 0; a < ctx->natoms; a++)
+    for (int d = 0; d < 3; d++) p.pos[3 * a + d] = ctx->motif[4 * a + d];
+  const size_t vbytes = (size_t)3 * N * sizeof(cd);
+  const size_t xbytes = (size_t)N * nstates * sizeof(cd);
+  XATU_CK(ctx->dv_R.ensure(vbytes));
+  XATU_CK(ctx->dv_tmp.ensure(xbytes + 64 * (size_t)nstates));
+  XATU_CK(ctx->dv_small.ensure((size_t)3 * nstates * sizeof(cd)));
+  const size_t smem = (2 * (size_t)p.norb * p.norb + p.nR + (size_t)p.nb * p.norb) * sizeof(cd) + p.nb * sizeof(double);
+  XATU_CK(cudaFuncSetAttribute(vme_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  vme_kernel<<<ctx->nk, 256, smem, ctx->stream>>>(p, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(),
+                                                  ctx->d_HR.as<cd>(), ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr,
+                                                  ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
+                                                  ctx->dv_R.as<cd>());
+  ctx->launches++;
+  XATU_CK(cudaGetLastError());
+  XATU_CK(cudaMemcpyAsync(ctx->dv_tmp.p, eigvec, xbytes, cudaMemcpyHostToDevice, ctx->stream));
+  exciton_vme_kernel<<<3 * nstates, 256, 0, ctx->stream>>>(ctx->dv_R.as<cd>(), ctx->dv_tmp.as<cd>(), (int)N, nstates,
+                                                           ctx->dv_small.as<cd>());
+  ctx->launches++;
+  XATU_CK(cudaGetLastError());
+  XATU_CK(cudaMemcpyAsync(vme_ex, ctx->dv_small.p, (size_t)3 * nstates * sizeof(cd), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  XATU_CK(cudaStreamSynchronize(ctx->stream));
+  return XATU_OK;
+}

@@ -55,6 +55,7 @@ struct AsmInputs {
   const cd* exL;           // N x na
   const cd* exR;           // N x na
   int* status;             // device error word
+  const int* basis;        // NULL, or N x 3 (k, valence column, conduction index) of a caller-given basis
 };
 
 struct AsmOutputs {

@@ -305,6 +305,14 @@ class ExcitonTB:
         self._call("xatu_bse_build", prec)
         self._precision = precision
 
+    def BShamiltonianBasis(self, basis, precision: str = "fp64"):
+        """ExcitonTB::BShamiltonian(const arma::imat& basis): H over the given e-h states,
+        rows {valence band, conduction band, k index} (absolute band numbers)."""
+        prec = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}[precision]
+        b = np.ascontiguousarray(np.asarray(basis, dtype=np.int32).reshape(-1, 3))
+        self._call("xatu_bse_build_basis", prec, b.shape[0], L.ptr(b))
+        self._precision = precision
+
     @property
     def HBS(self) -> np.ndarray:
         """The assembled matrix copied to the host (row-major complex128)."""
@@ -334,6 +342,16 @@ class ExcitonTB:
             self._call("xatu_bse_solve", L.SOLVER_DAVIDSON, nstates, L.ptr(ev), L.ptr(vec))
             return ResultTB(self, ev, None if vec is None else vec.T.copy())
         raise ValueError(f"unknown method {method}")
+
+    def excitonOscillatorStrength(self, eigvec: np.ndarray) -> np.ndarray:
+        """ResultTB::excitonOscillatorStrength (ResultTB.cpp:242-298): 3 x nstates velocity
+        matrix elements (atomic units) of the excitons in the columns of ``eigvec``."""
+        X = np.asfortranarray(np.asarray(eigvec, dtype=np.complex128))
+        if X.ndim == 1:
+            X = X[:, None]
+        out = np.zeros((3, X.shape[1]), dtype=np.complex128, order="F")
+        self._call("xatu_oscillator_strength", X.shape[1], L.ptr(X), L.ptr(out))
+        return out
 
     def davidsonConfig(self, tol: float = 0.0, max_iter: int = 0, block: int = 0):
         self._call("xatu_davidson_config", float(tol), int(max_iter), int(block))
