@@ -327,14 +327,12 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   bp.max_sweeps = 40;
   bp.has_overlap = ctx->has_overlap ? 1 : 0;
   bp.is_au = ctx->is_au ? 1 : 0;
-  const size_t per_warp = band_solve_smem_per_warp(ctx->norb, ctx->nR, bp.has_overlap);
-  int warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / per_warp));
-  const size_t smem = per_warp * warps;
+  const size_t smem = band_solve_smem(ctx->norb, ctx->nR, bp.has_overlap);
   XATU_CK(cudaFuncSetAttribute(band_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = (ctx->nk + warps - 1) / warps;
+  const int grid = ctx->nk, threads = 128;
   XATU_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
   const cd* SR = ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr;
-  band_solve_kernel<<<grid, 32 * warps, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
+  band_solve_kernel<<<grid, threads, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
                                                              ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                              ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
                                                              ctx->d_status.as<int>());
@@ -342,7 +340,7 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   XATU_CK(cudaGetLastError());
   if (ctx->qnonzero) {
     for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
-    band_solve_kernel<<<grid, 32 * warps, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
+    band_solve_kernel<<<grid, threads, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
                                                                ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                                ctx->d_eigvalQ.as<double>(), ctx->d_eigvecQ.as<cd>(),
                                                                ctx->d_status.as<int>());

@@ -13,6 +13,6 @@ extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb
                                                    cd* L, cd* R);
 extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoints, const double* cellsR, const cd* HR,
                                              const cd* SR, double* eigval, cd* eigvec, int* status);
-extern "C" size_t band_solve_smem_per_warp(int norb, int nR, int has_overlap);
+extern "C" size_t band_solve_smem(int norb, int nR, int has_overlap);
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path);
