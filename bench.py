@@ -42,7 +42,7 @@ WORKLOAD = dict(model="synthetic hexagonal 8+7+7 orbitals (seed 1234)", ncell=60
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=40)
+    p.add_argument("--steps", type=int, default=150)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--ncell", type=int, default=WORKLOAD["ncell"])
@@ -90,7 +90,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
@@ -235,6 +235,7 @@ def run_engine(args):
     torch.cuda.synchronize()
     launches0 = ex.kernelLaunches()
     clk = ClockSampler(local)
+    time.sleep(0.5)   # let nvidia-smi start sampling before the timed region
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

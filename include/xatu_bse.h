@@ -183,6 +183,25 @@ xatu_status xatu_kernel_matvec(xatu_ctx *ctx, int nvec, const double *X, double 
    modified in place. */
 xatu_status xatu_oscillator_strength(xatu_ctx *ctx, int nstates, const double *eigvec, double *vme_ex);
 
+/* ------------------------------------------------------------------ adjoint gradients */
+#define XATU_ADJOINT_MAX_STATES 8
+/* Hellmann-Feynman gradients dE_n/dtheta = x_n^H (dH/dtheta) x_n of exciton energies through the whole path
+   (band solve, fixGlobalPhase, interaction tables, BShamiltonian).  No reference counterpart: the reference has
+   no derivative code; this differentiates what ExcitonTB::initializeHamiltonian / BShamiltonian compute
+   (ExcitonTB.cpp:673-683, 707-921; SystemTB.cpp:60-156).
+   eigvec: host, N x nstates complex, column-major, normalised eigenvectors of the current build (for example
+   those returned by xatu_bse_solve); nstates <= XATU_ADJOINT_MAX_STATES.  The band eigenvectors are
+   recomputed on the device, not stored.
+   grad_hamiltonian (or NULL): nstates x nR x norb x norb complex, G_n(R)_ab = dE_n/dRe H(R)_ab + i dE_n/dIm H(R)_ab
+   for perturbations that keep H(k) Hermitian (with full storage, perturb H(R)_ab and H(-R)_ba = conj together;
+   the first-order change is dE = Re sum conj(G) dH).  Needs bands from xatu_bands_compute; undefined (and
+   XATU_ERR_NUMERIC) where a selected band is degenerate with another band.
+   grad_params (or NULL): nstates x 3 doubles, dE_n/dr0, dE_n/deps_m, dE_n/deps_s.
+   Supported: full e-h basis, at most 2 valence and 2 conduction bands, at most 4 atoms, both modes,
+   exchange, Q, overlap. */
+xatu_status xatu_adjoint(xatu_ctx *ctx, int nstates, const double *eigvec, double *grad_hamiltonian,
+                         double *grad_params);
+
 /* ------------------------------------------------------------------ instrumentation */
 /* Device milliseconds of the last run of each stage: [0] bands, [1] interaction tables, [2] assembly,
    [3] solve.  Measured with CUDA events on the context's stream. */

@@ -23,7 +23,7 @@ xatu_status xatu_cuda_fail(xatu_ctx* ctx, cudaError_t e, const char* where) {
   return xatu_fail(ctx, e == cudaErrorMemoryAllocation ? XATU_ERR_ALLOC : XATU_ERR_CUDA, m);
 }
 
-static xatu_status check_device_status(xatu_ctx* ctx, const char* stage) {
+xatu_status xatu_check_device_status(xatu_ctx* ctx, const char* stage) {
   int st = 0;
   XATU_CK(cudaMemcpyAsync(&st, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
@@ -34,7 +34,11 @@ static xatu_status check_device_status(xatu_ctx* ctx, const char* stage) {
   if (st & XATU_DEVERR_INDEX) m += " table index out of range;";
   if (st & XATU_DEVERR_NOCONV) m += " Jacobi sweep cap reached;";
   if (st & XATU_DEVERR_OVERLAP) m += " Zero or negative overlap eigenvalues found;";
-  return xatu_fail(ctx, (st & (XATU_DEVERR_NAN | XATU_DEVERR_OVERLAP)) ? XATU_ERR_NUMERIC : XATU_ERR_NOT_CONVERGED, m);
+  if (st & XATU_DEVERR_DEGEN)
+    m += " degenerate bands (or a zero coefficient sum) at a k point: the band eigenvector derivative is undefined;";
+  return xatu_fail(ctx, (st & (XATU_DEVERR_NAN | XATU_DEVERR_OVERLAP | XATU_DEVERR_DEGEN)) ? XATU_ERR_NUMERIC
+                                                                                           : XATU_ERR_NOT_CONVERGED,
+                   m);
 }
 
 template <typename T>
@@ -84,7 +88,9 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status,
                   &ctx->d_work, &ctx->dv_V, &ctx->dv_W, &ctx->dv_T, &ctx->dv_Y, &ctx->dv_U, &ctx->dv_R,
                   &ctx->dv_X, &ctx->dv_Yf, &ctx->dv_G, &ctx->dv_tmp, &ctx->dv_diagH, &ctx->dv_small,
-                  &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo};
+                  &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo, &ctx->d_adjX, &ctx->d_adjdvtab,
+                  &ctx->d_adjdtable, &ctx->d_adjdVX, &ctx->d_adjAlpha, &ctx->d_adjExUW, &ctx->d_adjCbar,
+                  &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG};
   for (DBuf* b : bufs) b->release();
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
@@ -353,11 +359,11 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
                             ctx->stream));
   }
   XATU_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-  xatu_status st = check_device_status(ctx, "band solve");
+  xatu_status st = xatu_check_device_status(ctx, "band solve");
   if (st != XATU_OK) return st;
   cudaEventElapsedTime(&ctx->stage_ms[0], ctx->ev[0], ctx->ev[1]);
   ctx->bands_ok = true;
-  ctx->tables_ok = ctx->tables_ok && true;
+  ctx->bands_from_model = true;
   ctx->built_prec = -1;
   return XATU_OK;
 }
@@ -376,6 +382,7 @@ xatu_status xatu_bands_upload(xatu_ctx* ctx, const double* eigval, const double*
   XATU_CK(upload(ctx->d_eigvecQ, eigvecQ ? eigvecQ : eigvec, 2 * nk * nb * norb, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   ctx->bands_ok = true;
+  ctx->bands_from_model = false;
   ctx->built_prec = -1;
   return XATU_OK;
 }
@@ -445,7 +452,7 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
     XATU_CK(ctx->d_table.ensure((size_t)ctx->nmesh * na * na * sizeof(cd)));
     const long long tot = (long long)npairs * ncells;
     int grid = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
-    pair_potential_kernel<<<grid, 256, 0, ctx->stream>>>(pp, ctx->potential, na, ctx->d_motif.as<double>(), ncells,
+    pair_potential_kernel<<<grid, 256, 0, ctx->stream>>>(pp, ctx->potential, 0, na, ctx->d_motif.as<double>(), ncells,
                                                          ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
                                                          ctx->d_vtab.as<double>());
     ctx->launches++;
@@ -461,7 +468,7 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
       const double* vt = ctx->d_vtab.as<double>();
       if (ctx->exchange_potential != ctx->potential) {
         XATU_CK(ctx->d_vtabX.ensure((size_t)npairs * ncells * sizeof(double)));
-        pair_potential_kernel<<<grid, 256, 0, ctx->stream>>>(pp, ctx->exchange_potential, na,
+        pair_potential_kernel<<<grid, 256, 0, ctx->stream>>>(pp, ctx->exchange_potential, 0, na,
                                                              ctx->d_motif.as<double>(), ncells,
                                                              ctx->d_cells.as<double>(), npairs,
                                                              ctx->d_pairs.as<int2>(), ctx->d_vtabX.as<double>());
@@ -483,13 +490,13 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
     XATU_CK(ctx->d_table.ensure((size_t)ctx->rt_entries * na * na * sizeof(cd)));
     const long long tot = ctx->rt_entries * na;
     int grid = (int)std::min<long long>((tot + 127) / 128, 148 * 32);
-    recip_table_kernel<<<grid, 128, 0, ctx->stream>>>(pp, t, (int)ctx->rt_entries, ctx->d_G.as<double>(), na,
+    recip_table_kernel<<<grid, 128, 0, ctx->stream>>>(pp, t, 0, (int)ctx->rt_entries, ctx->d_G.as<double>(), na,
                                                       ctx->d_motif.as<double>(), ctx->d_table.as<cd>());
     ctx->launches++;
     XATU_CK(cudaGetLastError());
     if (ctx->exchange) {
       const RecipTable tx = recip_table(ctx, true);
-      recip_table_kernel<<<1, 128, 0, ctx->stream>>>(pp, tx, 1, ctx->d_G.as<double>(), na, ctx->d_motif.as<double>(),
+      recip_table_kernel<<<1, 128, 0, ctx->stream>>>(pp, tx, 0, 1, ctx->d_G.as<double>(), na, ctx->d_motif.as<double>(),
                                                      ctx->d_VX.as<cd>());
       ctx->launches++;
       XATU_CK(cudaGetLastError());
@@ -633,7 +640,7 @@ static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis) {
   ctx->launches++;
   ctx->last_assembly_path = path;
   XATU_CK(cudaEventRecord(ctx->ev[5], ctx->stream));
-  st = check_device_status(ctx, "BSE assembly");
+  st = xatu_check_device_status(ctx, "BSE assembly");
   if (st != XATU_OK) return st;
   cudaEventElapsedTime(&ctx->stage_ms[2], ctx->ev[4], ctx->ev[5]);
   ctx->built_prec = precision;

@@ -38,22 +38,8 @@ __device__ __forceinline__ void split_store(__nv_bfloat162* hi, __nv_bfloat162* 
 }
 
 __device__ __forceinline__ const cd* interaction_ptr(const AsmParams& p, const AsmInputs& in, int k, int k2) {
-  int64_t e;
-  if (p.mode == 0) {
-    const double dx = in.kpoints[3 * k2] - in.kpoints[3 * k];
-    const double dy = in.kpoints[3 * k2 + 1] - in.kpoints[3 * k + 1];
-    const double dz = in.kpoints[3 * k2 + 2] - in.kpoints[3 * k + 2];
-    e = equivalent_index(p.emap, dx, dy, dz);
-  } else {
-    e = 0;
-    int64_t stride = 1;
-    for (int d = 0; d < p.rt_ndim; d++) {
-      const int off = in.kgrid[3 * k + d] - in.kgrid[3 * k2 + d];
-      e += (int64_t)(off + p.rt_span[d]) * stride;
-      stride *= p.rt_len[d];
-    }
-  }
-  if (e < 0 || e >= p.nentries) {
+  int64_t e = interaction_entry(p, in.kpoints, in.kgrid, k, k2);
+  if (e < 0) {
     atomicOr(in.status, XATU_DEVERR_INDEX);
     e = 0;
   }

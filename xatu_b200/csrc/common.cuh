@@ -93,6 +93,58 @@ __host__ __device__ inline double struve_h0(double x) {
   return 2.0 / (XATU_PI * x) * s + by0;
 }
 
+// Derivative d/dx of struve_h0: the exact derivative of the same truncated
+// approximation (same branch, same number of series terms), so that it is
+// consistent with finite differences of struve_h0 itself.
+//   x <= 20:  H0 = (2/pi) sum_k r_k x,    r_k ~ x^{2k}   ->  H0' = (2/pi) sum_k (2k+1) r_k
+//   x  > 20:  A  = (2/pi) sum_k r_k / x,  r_k ~ x^{-2k}  ->  A'  = -(2/pi) sum_k (2k+1) r_k / x^2
+//             by0 = 2 x^{-1/2} (p0 sin th + q0 cos th), th = x - pi/4, p0 = P(t^2),
+//             q0 = t Qp(t^2), t = 4/x, differentiated term by term.
+__host__ __device__ inline double struve_h0_dx(double x) {
+  double s = 1.0, r = 1.0, sk = 0.0;   // sk = sum_k k r_k
+  if (x <= 20.0) {
+    for (int k = 1; k < 61; k++) {
+      const double d = 2.0 * k + 1.0;
+      r = -r * x / d * x / d;
+      s += r;
+      sk += k * r;
+      if (fabs(r) < fabs(s) * 1.0e-12) break;
+    }
+    return (2.0 / XATU_PI) * (s + 2.0 * sk);
+  }
+  int km = (int)(0.5 * (x + 1.0));
+  if (x >= 50.0) km = 25;
+  for (int k = 1; k <= km; k++) {
+    const double u = (2.0 * k - 1.0) / x;
+    r = -r * (u * u);
+    s += r;
+    sk += k * r;
+    if (fabs(r) < fabs(s) * 1.0e-12) break;
+  }
+  const double dA = -(2.0 / (XATU_PI * x * x)) * (s + 2.0 * sk);
+  const double t = 4.0 / x, t2 = t * t;
+  const double P = ((((-.37043e-5 * t2 + .173565e-4) * t2 - .487613e-4) * t2 + .17343e-3) * t2 - 0.1753062e-2) * t2 +
+                   .3989422793;
+  const double dP = (((5.0 * -.37043e-5 * t2 + 4.0 * .173565e-4) * t2 - 3.0 * .487613e-4) * t2 + 2.0 * .17343e-3) * t2 -
+                    0.1753062e-2;
+  const double Qp = ((((.32312e-5 * t2 - 0.142078e-4) * t2 + 0.342468e-4) * t2 - 0.869791e-4) * t2 + 0.4564324e-3) * t2 -
+                    0.0124669441;
+  const double dQp = (((5.0 * .32312e-5 * t2 - 4.0 * 0.142078e-4) * t2 + 3.0 * 0.342468e-4) * t2 - 2.0 * 0.869791e-4) *
+                         t2 +
+                     0.4564324e-3;
+  const double dt2 = -2.0 * t2 / x;   // d(t^2)/dx
+  const double q0 = t * Qp;
+  const double dp0 = dP * dt2;
+  const double dq0 = (-t / x) * Qp + t * dQp * dt2;
+  const double th = x - 0.25 * XATU_PI;
+  const double sn = sin(th), cs = cos(th);
+  const double g = P * sn + q0 * cs;
+  const double dg = dp0 * sn + P * cs + dq0 * cs - q0 * sn;
+  const double rs = 1.0 / sqrt(x);
+  const double dby0 = -rs / x * g + 2.0 * rs * dg;
+  return dA + dby0;
+}
+
 // Keldysh potential V(r) in eV (ExcitonTB::keldysh semantics, ExcitonTB.cpp:347-366):
 // r = 0 uses the regularisation distance, r beyond |a1| * cutoff + 1e-5 is zero.
 __device__ inline double keldysh_potential(const PotParams& p, double r) {
@@ -106,6 +158,27 @@ __device__ inline double keldysh_potential(const PotParams& p, double r) {
   if (r > rc) return 0.0;
   const double x = fabs(r) / p.r0;
   return pref * (struve_h0(x) - y0(x));
+}
+
+// dV/dr0 of keldysh_potential.  With P = ec / (8e-10 eps0 eps_bar), rho = r (or
+// the regularisation distance at r = 0) and x = rho / r0:
+//   V = P / r0 f(x),  f = H0 - Y0,  f' = H0' + Y1
+//   dV/dr0 = -P / r0^2 (f(x) + x f'(x)).
+// (dV/deps_m = dV/deps_s = -V / (2 eps_bar) needs no table.)
+__device__ inline double keldysh_potential_dr0(const PotParams& p, double r) {
+  const double eps_bar = (p.eps_m + p.eps_s) / 2;
+  const double rc = p.a1norm * p.cutoff + 1E-5;
+  const double pref = XATU_EC / (8E-10 * XATU_EPS0 * eps_bar * p.r0 * p.r0);
+  double x;
+  if (r == 0) {
+    x = p.regularization / p.r0;
+  } else {
+    if (r > rc) return 0.0;
+    x = fabs(r) / p.r0;
+  }
+  const double f = struve_h0(x) - y0(x);
+  const double df = struve_h0_dx(x) + y1(x);
+  return -pref * (f + x * df);
 }
 
 // Coulomb potential in eV (ExcitonTB::coulomb semantics, ExcitonTB.cpp:374-381).
@@ -124,6 +197,16 @@ __device__ inline double keldysh_ft(const PotParams& p, double qx, double qy, do
   const double qn = sqrt(qx * qx + qy * qy + qz * qz);
   const double v = (qn < eps) ? 0.0 : 1 / (qn * (1 + p.r0 * qn));
   return v * XATU_EC * 1E10 / (2 * XATU_EPS0 * eps_bar * p.area * p.total_cells);
+}
+
+// dVt/dr0 of keldysh_ft: Vt ~ 1 / (|q| (1 + r0 |q|))  ->  dVt/dr0 = -Vt |q| / (1 + r0 |q|).
+__device__ inline double keldysh_ft_dr0(const PotParams& p, double qx, double qy, double qz) {
+  const double eps_bar = (p.eps_m + p.eps_s) / 2;
+  const double eps = p.b1norm / p.total_cells;
+  const double qn = sqrt(qx * qx + qy * qy + qz * qz);
+  if (qn < eps) return 0.0;
+  const double d = 1 + p.r0 * qn;
+  return -1.0 / (d * d) * XATU_EC * 1E10 / (2 * XATU_EPS0 * eps_bar * p.area * p.total_cells);
 }
 
 // ----------------------------------------------------------------- k-difference -> mesh index
@@ -161,4 +244,11 @@ __device__ __forceinline__ int equivalent_index(const EquivMap& m, double dx, do
 // ----------------------------------------------------------------- error flag
 // Kernels never trap: out-of-contract indices are recorded in a device word the
 // host reads after the stage.
-enum { XATU_DEVERR_NONE = 0, XATU_DEVERR_INDEX = 1, XATU_DEVERR_NAN = 2, XATU_DEVERR_NOCONV = 4, XATU_DEVERR_OVERLAP = 8 };
+enum {
+  XATU_DEVERR_NONE = 0,
+  XATU_DEVERR_INDEX = 1,
+  XATU_DEVERR_NAN = 2,
+  XATU_DEVERR_NOCONV = 4,
+  XATU_DEVERR_OVERLAP = 8,
+  XATU_DEVERR_DEGEN = 16   // degenerate band pair where an eigenvector derivative is needed
+};

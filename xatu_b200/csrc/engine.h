@@ -41,7 +41,7 @@ struct xatu_ctx {
   long long launches = 0;
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
-  cudaEvent_t ev[10] = {};
+  cudaEvent_t ev[12] = {};
   float stage_ms[4] = {0, 0, 0, 0};
 
   // ---------------- system
@@ -94,11 +94,19 @@ struct xatu_ctx {
   int dav_iters = 0;
   double dav_maxres = 0;
   DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo;
+
+  // ---------------- adjoint
+  bool bands_from_model = false;   // bands came from xatu_bands_compute (not uploaded)
+  float adjoint_ms = 0;
+  DBuf d_adjX, d_adjdvtab, d_adjdtable, d_adjdVX, d_adjAlpha, d_adjExUW, d_adjCbar, d_adjEbar, d_adjEpart, d_adjGk,
+      d_adjG;
 };
 
 // status helpers
 xatu_status xatu_fail(xatu_ctx* ctx, xatu_status code, const std::string& msg);
 xatu_status xatu_cuda_fail(xatu_ctx* ctx, cudaError_t e, const char* where);
+// Reads and clears the device error word; maps its flags to a status and message.
+xatu_status xatu_check_device_status(xatu_ctx* ctx, const char* stage);
 
 // launchers implemented in the .cu files
 struct AsmParams;

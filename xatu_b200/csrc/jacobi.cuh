@@ -191,123 +191,6 @@ __device__ int jacobi_eigh(const G& g, cd* A, int lda, cd* V, int ldv, int n, Ja
   return sweep;
 }
 
-// One-warp variant for the batched band solve.  Same rotations and ordering as
-// jacobi_eigh, but each round runs as lane-per-row / lane-per-column passes
-// instead of 2x2 block tasks: the column rotations (and the eigenvector update)
-// walk the rows of A and V with one lane per row, the row rotations walk the
-// columns with one lane per column.  With an odd row pitch every shared-memory
-// access of a pass is bank-conflict free, and the rotation table is read as a
-// broadcast.  Three warp barriers per round.
-__device__ inline int jacobi_eigh_warp(cd* A, int lda, cd* V, int ldv, int n, JacobiRot* rot, int max_sweeps,
-                                       double rel_tol) {
-  const int lane = threadIdx.x & 31;
-  for (int r = lane; r < n; r += 32) {
-    for (int c = 0; c < n; c++) V[r * ldv + c] = mk(r == c ? 1.0 : 0.0, 0.0);
-    A[r * lda + r].y = 0.0;
-  }
-  __syncwarp();
-  if (n <= 1) return 0;
-  const int n2 = n + (n & 1);
-  const int m = n2 - 1;
-  const int np = n2 / 2;
-  int sweep = 0;
-  for (; sweep <= max_sweeps; sweep++) {
-    double off = 0.0, tot = 0.0;
-    for (int r = lane; r < n; r += 32)
-      for (int c = 0; c < n; c++) {
-        const double a2 = nrm2(A[r * lda + c]);
-        tot += a2;
-        if (r != c) off += a2;
-      }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      off += __shfl_xor_sync(0xffffffffu, off, o);
-      tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    }
-    if (off <= rel_tol * rel_tol * tot || off == 0.0) break;
-    if (sweep == max_sweeps) {
-      sweep++;
-      break;
-    }
-    for (int r = 0; r < m; r++) {
-      for (int i = lane; i < np; i += 32) {
-        int a, b;
-        if (i == 0) {
-          a = r;
-          b = m;
-        } else {
-          a = r + i;
-          if (a >= m) a -= m;
-          b = r - i;
-          if (b < 0) b += m;
-        }
-        JacobiRot R;
-        R.p = min(a, b);
-        R.q = max(a, b);
-        R.rot = 0;
-        R.cs = 1.0;
-        R.se = mk(0, 0);
-        R.app = R.aqq = 0.0;
-        if (R.q < n) {
-          const cd c = A[R.p * lda + R.q];
-          const double ac = sqrt(nrm2(c));
-          if (ac > 1e-300) {
-            const double app = A[R.p * lda + R.p].x, aqq = A[R.q * lda + R.q].x;
-            const double tau = (aqq - app) / (2.0 * ac);
-            const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            const double cs = 1.0 / sqrt(1.0 + t * t);
-            const double sn = t * cs;
-            R.cs = cs;
-            R.se = mk(sn * c.x / ac, sn * c.y / ac);
-            R.app = app - t * ac;
-            R.aqq = aqq + t * ac;
-            R.rot = 1;
-          }
-        }
-        rot[i] = R;
-      }
-      __syncwarp();
-      // column pass: A <- A J and V <- V J, one lane per row
-      for (int row = lane; row < n; row += 32) {
-        for (int i = 0; i < np; i++) {
-          const JacobiRot& R = rot[i];
-          if (!R.rot) continue;
-          cd x = A[row * lda + R.p], y = A[row * lda + R.q];
-          rot_right(R, x, y);
-          A[row * lda + R.p] = x;
-          A[row * lda + R.q] = y;
-          cd vx = V[row * ldv + R.p], vy = V[row * ldv + R.q];
-          rot_right(R, vx, vy);
-          V[row * ldv + R.p] = vx;
-          V[row * ldv + R.q] = vy;
-        }
-      }
-      __syncwarp();
-      // row pass: A <- J^H A, one lane per column; the 2x2 pivot blocks get their exact form
-      for (int col = lane; col < n; col += 32) {
-        for (int i = 0; i < np; i++) {
-          const JacobiRot& R = rot[i];
-          if (!R.rot) continue;
-          if (col == R.p) {
-            A[R.p * lda + col] = mk(R.app, 0);
-            A[R.q * lda + col] = mk(0, 0);
-          } else if (col == R.q) {
-            A[R.q * lda + col] = mk(R.aqq, 0);
-            A[R.p * lda + col] = mk(0, 0);
-          } else {
-            cd x = A[R.p * lda + col], y = A[R.q * lda + col];
-            rot_left(R, x, y);
-            A[R.p * lda + col] = x;
-            A[R.q * lda + col] = y;
-          }
-        }
-      }
-      __syncwarp();
-    }
-  }
-  return sweep;
-}
-
 // Ascending order of the eigenvalues (diagonal of A): perm[rank] = index.
 template <class G>
 __device__ void jacobi_sort(const G& g, const cd* A, int lda, int n, int* perm) {

@@ -2,12 +2,13 @@
 #pragma once
 #include "params.h"
 
-extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int na, const double* motif, int ncells,
-                                                 const double* cells, int npairs, const int2* pairs, double* vtab);
+extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int deriv, int na, const double* motif,
+                                                 int ncells, const double* cells, int npairs, const int2* pairs,
+                                                 double* vtab);
 extern "C" __global__ void motif_ft_kernel(int nq, const double* q, int ncells, const double* cells, int npairs,
                                            const int2* pairs, const double* vtab, double inv_total, int na, cd* out);
-extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nentries, const double* G, int na,
-                                              const double* motif, cd* W);
+extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int deriv, int nentries, const double* G,
+                                              int na, const double* motif, cd* W);
 extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na, const int* orb_off,
                                                    const cd* eigvec, const cd* eigvecQ, const cd* VX, const int* basis,
                                                    cd* L, cd* R);

@@ -25,8 +25,10 @@
 #define MOTIF_PAIR_CHUNK 8
 #define MOTIF_THREADS 256
 
-extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int na, const double* __restrict__ motif,
-                                                 int ncells, const double* __restrict__ cells, int npairs,
+// deriv = 0: V itself; deriv = 1: dV/dr0 (zero for the Coulomb potential).
+extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int deriv, int na,
+                                                 const double* __restrict__ motif, int ncells,
+                                                 const double* __restrict__ cells, int npairs,
                                                  const int2* __restrict__ pairs, double* __restrict__ vtab) {
   const int64_t total = (int64_t)npairs * ncells;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
@@ -40,7 +42,10 @@ extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int na, 
     const double d1 = c[1] + ta[1] - tb[1];
     const double d2 = c[2] + ta[2] - tb[2];
     const double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-    vtab[t] = (kind == 1) ? coulomb_potential(p, r) : keldysh_potential(p, r);
+    if (deriv)
+      vtab[t] = (kind == 1) ? 0.0 : keldysh_potential_dr0(p, r);
+    else
+      vtab[t] = (kind == 1) ? coulomb_potential(p, r) : keldysh_potential(p, r);
   }
 }
 
@@ -97,8 +102,10 @@ motif_ft_kernel(int nq, const double* __restrict__ q, int ncells, const double* 
   }
 }
 
-extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nentries, const double* __restrict__ G,
-                                              int na, const double* __restrict__ motif, cd* __restrict__ W) {
+// deriv = 0: W itself; deriv = 1: dW/dr0.
+extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int deriv, int nentries,
+                                              const double* __restrict__ G, int na, const double* __restrict__ motif,
+                                              cd* __restrict__ W) {
   const int64_t total = (int64_t)nentries * na;
   for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < total;
        id += (int64_t)gridDim.x * blockDim.x) {
@@ -119,7 +126,7 @@ extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int nen
     const double tax = motif[4 * a], tay = motif[4 * a + 1], taz = motif[4 * a + 2];
     for (int g = 0; g < t.nG; g++) {
       const double gx = qx + G[3 * g], gy = qy + G[3 * g + 1], gz = qz + G[3 * g + 2];
-      const double v = keldysh_ft(p, gx, gy, gz);
+      const double v = deriv ? keldysh_ft_dr0(p, gx, gy, gz) : keldysh_ft(p, gx, gy, gz);
       if (v == 0.0) continue;
       for (int b = 0; b < na; b++) {
         const double ph = gx * (tax - motif[4 * b]) + gy * (tay - motif[4 * b + 1]) + gz * (taz - motif[4 * b + 2]);

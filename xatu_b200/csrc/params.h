@@ -65,3 +65,29 @@ struct AsmOutputs {
   double* diag;            // MIXED: N
 };
 
+
+// Row of the interaction table for the pair (k, k2) of exciton k points:
+// real space: the mesh point equivalent to k2 - k (findEquivalentPointBZ);
+// reciprocal space: the integer grid offset k - k2.  P needs the members
+// mode, emap, rt_ndim, rt_len, rt_span and nentries.  Returns -1 when the entry
+// falls outside the table.
+template <class P>
+__device__ __forceinline__ int64_t interaction_entry(const P& p, const double* __restrict__ kpoints,
+                                                     const int* __restrict__ kgrid, int k, int k2) {
+  int64_t e;
+  if (p.mode == 0) {
+    const double dx = kpoints[3 * k2] - kpoints[3 * k];
+    const double dy = kpoints[3 * k2 + 1] - kpoints[3 * k + 1];
+    const double dz = kpoints[3 * k2 + 2] - kpoints[3 * k + 2];
+    e = equivalent_index(p.emap, dx, dy, dz);
+  } else {
+    e = 0;
+    int64_t stride = 1;
+    for (int d = 0; d < p.rt_ndim; d++) {
+      const int off = kgrid[3 * k + d] - kgrid[3 * k2 + d];
+      e += (int64_t)(off + p.rt_span[d]) * stride;
+      stride *= p.rt_len[d];
+    }
+  }
+  return (e < 0 || e >= p.nentries) ? -1 : e;
+}

@@ -353,6 +353,30 @@ class ExcitonTB:
         self._call("xatu_oscillator_strength", X.shape[1], L.ptr(X), L.ptr(out))
         return out
 
+    def adjointGradients(self, eigvec: np.ndarray, hamiltonian: bool = True, params: bool = True) -> dict:
+        """Hellmann-Feynman gradients of the exciton energies of the normalised eigenvectors in the
+        columns of ``eigvec`` (at most 8), through bands, interaction tables and assembly.
+
+        Returns ``{"hamiltonian": G, "r0": ..., "eps_m": ..., "eps_s": ...}``: G has shape
+        (nstates, nR, norb, norb) with G[n, R] = dE_n/dRe H(R) + i dE_n/dIm H(R) for perturbations that keep
+        H(k) Hermitian (dE = Re sum conj(G) dH); the others have shape (nstates,)."""
+        X = np.asfortranarray(np.asarray(eigvec, dtype=np.complex128))
+        if X.ndim == 1:
+            X = X[:, None]
+        ns = X.shape[1]
+        s = self.system
+        G = np.zeros((ns, s.hamiltonianMatrices.shape[0], s.basisdim, s.basisdim), dtype=np.complex128) \
+            if hamiltonian else None
+        P = np.zeros((ns, 3)) if params else None
+        self._call("xatu_adjoint", ns, L.ptr(X), L.ptr(G) if G is not None else None,
+                   L.ptr(P) if P is not None else None)
+        out = {}
+        if G is not None:
+            out["hamiltonian"] = G
+        if P is not None:
+            out["r0"], out["eps_m"], out["eps_s"] = P[:, 0].copy(), P[:, 1].copy(), P[:, 2].copy()
+        return out
+
     def davidsonConfig(self, tol: float = 0.0, max_iter: int = 0, block: int = 0):
         self._call("xatu_davidson_config", float(tol), int(max_iter), int(block))
 
