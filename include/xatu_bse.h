@@ -202,12 +202,40 @@ xatu_status xatu_oscillator_strength(xatu_ctx *ctx, int nstates, const double *e
 xatu_status xatu_adjoint(xatu_ctx *ctx, int nstates, const double *eigvec, double *grad_hamiltonian,
                          double *grad_params);
 
+/* ------------------------------------------------------------------ batches of systems */
+/* Many BSE instances of uneven size (k grids, band windows, dielectric parameters) built and solved together
+   on one GPU.  No reference counterpart (the reference handles one ExcitonTB at a time); each member follows
+   initializeHamiltonian + BShamiltonian(mixed) + diagonalize("davidson") of one system.  The first
+   xatu_batch_run tunes the assembly tile of each band-window class on the batch's own data and records the
+   build (band solves, tables, one persistent assembly launch per class) and one step of a lockstep block
+   Davidson into CUDA graphs; later runs replay them.  Supported members: 1-3 valence and 1-3 conduction bands,
+   2-3 atoms, BSE dimension >= 64, lowest nstates <= 12 (block of at most 16 vectors). */
+typedef struct xatu_batch xatu_batch;
+xatu_status xatu_batch_create(xatu_batch **batch, int device);
+xatu_status xatu_batch_destroy(xatu_batch *batch);
+const char *xatu_batch_last_error(const xatu_batch *batch);
+/* cudaStream_t as void*, NULL = the batch's own stream; before the first run. */
+xatu_status xatu_batch_set_stream(xatu_batch *batch, void *stream);
+/* Adds one system (copies the descriptors' arrays, as xatu_system_upload + xatu_exciton_set); *index = its slot. */
+xatu_status xatu_batch_add(xatu_batch *batch, const xatu_system_desc *sys, const xatu_exciton_desc *exc, int *index);
+/* Builds and solves every member: lowest nstates, residual tolerance tol (<= 0: 1e-4), at most max_iter
+   Davidson steps (<= 0: 200).  nstates, tol and max_iter are fixed by the first run. */
+xatu_status xatu_batch_run(xatu_batch *batch, int nstates, double tol, int max_iter);
+xatu_status xatu_batch_dim(const xatu_batch *batch, int index, int64_t *n);
+/* eigval: nstates; eigvec: N x nstates complex, column-major (either may be NULL). */
+xatu_status xatu_batch_result(xatu_batch *batch, int index, double *eigval, double *eigvec);
+/* Device ms of the last run's build graph and Davidson iterations, the number of lockstep iterations, the
+   iterations each member needed (array of the batch size, or NULL) and the autotuner's choices as JSON text. */
+xatu_status xatu_batch_stats(const xatu_batch *batch, double *build_ms, double *solve_ms, int *iterations,
+                             int *member_iterations, char *tuning, size_t tuning_len);
+
 /* ------------------------------------------------------------------ instrumentation */
 /* Device milliseconds of the last run of each stage: [0] bands, [1] interaction tables, [2] assembly,
    [3] solve.  Measured with CUDA events on the context's stream. */
 xatu_status xatu_stage_times(const xatu_ctx *ctx, float *ms4);
 /* Device time of one kernel family measured with CUDA events on the context's stream: which = 0 the BSE
-   assembly (last build), 1 the K.X products of the last Davidson solve.  *path: 1 CUDA cores, 2 tcgen05. */
+   assembly (last build), 1 the K.X products of the last Davidson solve, 2 the last xatu_adjoint call (first
+   to last launch), 3 its pair kernel.  *path: 1 CUDA cores, 2 tcgen05 (0 where it does not apply). */
 xatu_status xatu_kernel_stats(const xatu_ctx *ctx, int which, int64_t *launches, double *total_ms, int *path);
 /* Number of engine kernels launched on this context since creation. */
 xatu_status xatu_kernel_launches(const xatu_ctx *ctx, int64_t *count);

@@ -30,7 +30,9 @@ EXPORTED_SYMBOLS = [
     "xatu_interaction_build", "xatu_motif_ft_download", "xatu_bse_build", "xatu_bse_dim", "xatu_bse_copy_to_host",
     "xatu_bse_device_buffers", "xatu_bse_solve", "xatu_davidson_config", "xatu_davidson_stats", "xatu_stage_times",
     "xatu_hx_backend", "xatu_kernel_matvec", "xatu_kernel_stats", "xatu_hx_noalloc", "xatu_oscillator_strength",
-    "xatu_bse_build_basis", "xatu_adjoint",
+    "xatu_bse_build_basis", "xatu_adjoint", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
+    "xatu_batch_set_stream", "xatu_batch_add", "xatu_batch_run", "xatu_batch_dim", "xatu_batch_result",
+    "xatu_batch_stats",
     "xatu_kernel_launches", "xatu_reciprocal_lattice", "xatu_mesh_mp", "xatu_mesh_reduced",
     "xatu_equivalent_points", "xatu_truncate_supercell",
 ]
@@ -101,6 +103,15 @@ def lib() -> ctypes.CDLL:
         "xatu_oscillator_strength": ([vp, ci, vp, vp], ci),
         "xatu_bse_build_basis": ([vp, ci, ctypes.c_int64, vp], ci),
         "xatu_adjoint": ([vp, ci, vp, vp, vp], ci),
+        "xatu_batch_create": ([vp, ci], ci),
+        "xatu_batch_destroy": ([vp], ci),
+        "xatu_batch_last_error": ([vp], ctypes.c_char_p),
+        "xatu_batch_set_stream": ([vp, vp], ci),
+        "xatu_batch_add": ([vp, vp, vp, vp], ci),
+        "xatu_batch_run": ([vp, ci, ctypes.c_double, ci], ci),
+        "xatu_batch_dim": ([vp, ci, i64p], ci),
+        "xatu_batch_result": ([vp, ci, vp, vp], ci),
+        "xatu_batch_stats": ([vp, vp, vp, vp, vp, vp, ctypes.c_size_t], ci),
         "xatu_kernel_launches": ([vp, i64p], ci),
         "xatu_reciprocal_lattice": ([ci, vp, vp], ci),
         "xatu_mesh_mp": ([ci, vp, ci, vp], ci),

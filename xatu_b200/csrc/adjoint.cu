@@ -94,12 +94,12 @@ template <int NV, int NC, int NA>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjInputs in, AdjOutputs out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NB = NV + NC;
-  constexpr int WC = NC * NA * NC, WN = WC + NV * NA * NV;
+  constexpr int WC = NC * NA * NC;   // wc elements per partner (wv: NV * NA * NV follow)
   const int norb = p.norb, ns = p.ns, k = blockIdx.x, tid = threadIdx.x;
   cd* Ck = reinterpret_cast<cd*>(smem_raw);    // NB x norb (valence rows from the k stack, conduction from k + Q)
   cd* xa = Ck + NB * norb;                     // ns x NC*NV
   cd* acc = xa + ns * NC * NV;                 // ns x NB x norb
-  cd* w = acc + ns * NB * norb;                // ADJ_THREADS x WN
+  cd* w = acc + ns * NB * norb;                // WN x ADJ_THREADS (element-major: conflict-free stores)
   __shared__ double eacc[8][2];
   __shared__ int atom_of[XATU_MAX_ORB];
 
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
       double eV = 0.0, eR = 0.0;
       if (valid) {
         const cd* xs = xa + s * (NC * NV);
-        cd* wt = w + tid * WN;
+        cd* wt = w + tid;   // element e of this partner at wt[e * ADJ_THREADS]
         cd xb[NC][NV];
 #pragma unroll
         for (int c2i = 0; c2i < NC; c2i++)
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
                 cd t = mk(0, 0);
 #pragma unroll
                 for (int c = 0; c < NC; c++) t = t + cmulc(xs[c * NV + v], PV[c][v2]);
-                wt[WC + (v * NA + b) * NV + v2] = mk(-t.x, t.y);   // -conj(t)
+                wt[(WC + (v * NA + b) * NV + v2) * ADJ_THREADS] = mk(-t.x, t.y);   // -conj(t)
               }
           }
         }
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
                   t = t + cmulc(xs[c * NV + v], B[c2i][v]);
                   u = u + cmulc(xs[c * NV + v], dB[c2i][v]);
                 }
-                wt[(c * NA + a) * NC + c2i] = mk(-t.x, -t.y);
+                wt[((c * NA + a) * NC + c2i) * ADJ_THREADS] = mk(-t.x, -t.y);
                 // Gamma-weighted sums: sum_c' P_a(c, c') (.)
                 const cd pt = P[a][c][c2i] * t, pu = P[a][c][c2i] * u;
                 eV += pt.x;
@@ -280,17 +280,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
         if (b >= NV) {
           const int c = b - NV;
           for (int q = 0; q < nq; q++) {
-            const cd* ww = w + q * WN + (c * NA + a) * NC;
+            const cd* ww = w + (c * NA + a) * NC * ADJ_THREADS + q;
             const cd* cq = in.eigvecQ + ((int64_t)(base + q) * p.nb + NV) * norb + o;
 #pragma unroll
-            for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i] * cq[c2i * norb];
+            for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_THREADS] * cq[c2i * norb];
           }
         } else {
           for (int q = 0; q < nq; q++) {
-            const cd* ww = w + q * WN + WC + (b * NA + a) * NV;
+            const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_THREADS + q;
             const cd* cv = in.eigvec + (int64_t)(base + q) * p.nb * norb + o;
 #pragma unroll
-            for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2] * cv[v2 * norb];
+            for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_THREADS] * cv[v2 * norb];
           }
         }
         acc[(s * NB + b) * norb + o] = acc[(s * NB + b) * norb + o] + sum;
@@ -565,8 +565,7 @@ adj_hop_kernel(int nk, int norb, int triangular, const double* __restrict__ kpoi
 template <int NV, int NC, int NA>
 static cudaError_t launch_pair(const AdjParams& p, const AdjInputs& in, const AdjOutputs& out, cudaStream_t st) {
   const size_t smem = adj_pair_smem(NV, NC, NA, p.norb, p.ns);
-  cudaError_t e = cudaFuncSetAttribute(adj_pair_kernel<NV, NC, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = xatu_raise_smem_limit((const void*)adj_pair_kernel<NV, NC, NA>, smem);
   if (e != cudaSuccess) return e;
   adj_pair_kernel<NV, NC, NA><<<p.nk, ADJ_THREADS, smem, st>>>(p, in, out);
   return cudaGetLastError();
@@ -651,10 +650,8 @@ extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* ei
                                                   ctx->d_adjdvtab.as<double>());
       ctx->launches++;
       XATU_CK(cudaGetLastError());
-      XATU_CK(ctx->d_work.ensure(3 * sizeof(double)));
-      XATU_CK(cudaMemcpyAsync(ctx->d_work.p, ctx->Q, 3 * sizeof(double), cudaMemcpyHostToDevice, st));
       dim3 g3(1, (npairs + 7) / 8);
-      motif_ft_kernel<<<g3, 256, 0, st>>>(1, ctx->d_work.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
+      motif_ft_kernel<<<g3, 256, 0, st>>>(1, ctx->d_Q.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
                                           ctx->d_pairs.as<int2>(), ctx->d_adjdvtab.as<double>(),
                                           1.0 / ctx->total_cells, na, ctx->d_adjdVX.as<cd>());
       ctx->launches++;
@@ -770,13 +767,16 @@ extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* ei
   out.cbar = ctx->d_adjCbar.as<cd>();
   out.ebar = ctx->d_adjEbar.as<double>();
   out.epart = ctx->d_adjEpart.as<double>();
+  XATU_CK(cudaEventRecord(ctx->ev[8], st));
   XATU_CK(launch_pair_any(p, in, out, st));
   ctx->launches++;
+  XATU_CK(cudaEventRecord(ctx->ev[9], st));
 
   // potential parameters
   std::vector<double> epart((size_t)nk * ns * 2);
   XATU_CK(cudaMemcpyAsync(epart.data(), out.epart, epart.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   XATU_CK(cudaStreamSynchronize(st));
+  cudaEventElapsedTime(&ctx->adj_pair_ms, ctx->ev[8], ctx->ev[9]);
   {
     xatu_status s0 = xatu_check_device_status(ctx, "adjoint pair sums");
     if (s0 != XATU_OK) return s0;
@@ -828,8 +828,7 @@ extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* ei
     const size_t smemQ = ctx->qnonzero ? adj_band_smem(norb, ctx->nR, bp.has_overlap, nb - ctx->nv) : 0;
     if (std::max(smem, smemQ) > 227 * 1024)
       return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "adjoint band kernel: orbital basis too large for shared memory");
-    XATU_CK(cudaFuncSetAttribute(adj_band_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)std::max(smem, smemQ)));
+    XATU_CK(xatu_raise_smem_limit((const void*)adj_band_kernel, std::max(smem, smemQ)));
     adj_band_kernel<<<nk, ADJ_BAND_THREADS, smem, st>>>(bp, ns, 0, r1, ctx->d_kpoints.as<double>(),
                                                         ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                         out.cbar, out.ebar, g0, ctx->d_status.as<int>());

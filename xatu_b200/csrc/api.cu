@@ -4,6 +4,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -39,6 +41,20 @@ xatu_status xatu_check_device_status(xatu_ctx* ctx, const char* stage) {
   return xatu_fail(ctx, (st & (XATU_DEVERR_NAN | XATU_DEVERR_OVERLAP | XATU_DEVERR_DEGEN)) ? XATU_ERR_NUMERIC
                                                                                            : XATU_ERR_NOT_CONVERGED,
                    m);
+}
+
+cudaError_t xatu_raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limits;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limits[std::make_pair(dev, kernel)];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
 }
 
 template <typename T>
@@ -83,7 +99,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   DBuf* bufs[] = {&ctx->d_motif, &ctx->d_orboff, &ctx->d_basis, &ctx->d_cellsR, &ctx->d_HR, &ctx->d_SR, &ctx->d_kpoints, &ctx->d_mesh,
-                  &ctx->d_cells, &ctx->d_G, &ctx->d_kgrid, &ctx->d_eigval, &ctx->d_eigvec, &ctx->d_eigvalQ,
+                  &ctx->d_cells, &ctx->d_G, &ctx->d_kgrid, &ctx->d_Q, &ctx->d_eigval, &ctx->d_eigvec, &ctx->d_eigvalQ,
                   &ctx->d_eigvecQ, &ctx->d_pairs, &ctx->d_vtab, &ctx->d_vtabX, &ctx->d_table, &ctx->d_VX,
                   &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status,
                   &ctx->d_work, &ctx->dv_V, &ctx->dv_W, &ctx->dv_T, &ctx->dv_Y, &ctx->dv_U, &ctx->dv_R,
@@ -307,16 +323,27 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
   XATU_CK(upload(ctx->d_cells, ctx->cells.data(), ctx->cells.size(), ctx->stream));
   XATU_CK(upload(ctx->d_G, ctx->G.data(), ctx->G.size(), ctx->stream));
   XATU_CK(upload(ctx->d_kgrid, ctx->kgrid.data(), ctx->kgrid.size(), ctx->stream));
+  {
+    std::vector<int2> pairs;
+    for (int a = 0; a < ctx->natoms; a++)
+      for (int b = a; b < ctx->natoms; b++) pairs.push_back(make_int2(a, b));
+    XATU_CK(upload(ctx->d_pairs, pairs.data(), pairs.size(), ctx->stream));
+    XATU_CK(upload(ctx->d_Q, ctx->Q, 3, ctx->stream));
+  }
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   ctx->has_exciton = true;
   return XATU_OK;
 }
 
 // ------------------------------------------------------------------ bands
-xatu_status xatu_bands_compute(xatu_ctx* ctx) {
-  if (!ctx) return XATU_ERR_INVALID;
-  cudaSetDevice(ctx->device);
-  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+// Band-solve kernels on the context's stream: no host synchronisation and no
+// host copies (so that the sequence can be recorded into a CUDA graph once the
+// buffers exist).
+xatu_status xatu_bands_enqueue(xatu_ctx* ctx) {
+  {
+    const cudaError_t pending = cudaGetLastError();
+    if (pending != cudaSuccess) return xatu_cuda_fail(ctx, pending, "an earlier call (pending before the band solve)");
+  }
   const size_t nk = ctx->nk, nb = ctx->nb, norb = ctx->norb;
   XATU_CK(ctx->d_eigval.ensure(nk * nb * sizeof(double)));
   XATU_CK(ctx->d_eigvec.ensure(nk * nb * norb * sizeof(cd)));
@@ -334,16 +361,15 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
   bp.has_overlap = ctx->has_overlap ? 1 : 0;
   bp.is_au = ctx->is_au ? 1 : 0;
   const size_t smem = band_solve_smem(ctx->norb, ctx->nR, bp.has_overlap);
-  XATU_CK(cudaFuncSetAttribute(band_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  XATU_CK(xatu_raise_smem_limit((const void*)band_solve_kernel, smem));
   const int grid = ctx->nk, threads = 128;
-  XATU_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
   const cd* SR = ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr;
   band_solve_kernel<<<grid, threads, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
                                                              ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
                                                              ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
                                                              ctx->d_status.as<int>());
   ctx->launches++;
-  XATU_CK(cudaGetLastError());
+  XATU_CK_LAUNCH("band_solve_kernel");
   if (ctx->qnonzero) {
     for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
     band_solve_kernel<<<grid, threads, smem, ctx->stream>>>(bp, ctx->d_kpoints.as<double>(),
@@ -351,15 +377,25 @@ xatu_status xatu_bands_compute(xatu_ctx* ctx) {
                                                                ctx->d_eigvalQ.as<double>(), ctx->d_eigvecQ.as<cd>(),
                                                                ctx->d_status.as<int>());
     ctx->launches++;
-    XATU_CK(cudaGetLastError());
+    XATU_CK_LAUNCH("band_solve_kernel (k+Q)");
   } else {
     XATU_CK(cudaMemcpyAsync(ctx->d_eigvalQ.p, ctx->d_eigval.p, nk * nb * sizeof(double), cudaMemcpyDeviceToDevice,
                             ctx->stream));
     XATU_CK(cudaMemcpyAsync(ctx->d_eigvecQ.p, ctx->d_eigvec.p, nk * nb * norb * sizeof(cd), cudaMemcpyDeviceToDevice,
                             ctx->stream));
   }
+  return XATU_OK;
+}
+
+xatu_status xatu_bands_compute(xatu_ctx* ctx) {
+  if (!ctx) return XATU_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+  XATU_CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+  xatu_status st = xatu_bands_enqueue(ctx);
+  if (st != XATU_OK) return st;
   XATU_CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-  xatu_status st = xatu_check_device_status(ctx, "band solve");
+  st = xatu_check_device_status(ctx, "band solve");
   if (st != XATU_OK) return st;
   cudaEventElapsedTime(&ctx->stage_ms[0], ctx->ev[0], ctx->ev[1]);
   ctx->bands_ok = true;
@@ -432,21 +468,14 @@ static RecipTable recip_table(const xatu_ctx* ctx, bool single_q) {
   return t;
 }
 
-xatu_status xatu_interaction_build(xatu_ctx* ctx) {
-  if (!ctx) return XATU_ERR_INVALID;
-  cudaSetDevice(ctx->device);
-  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+// Interaction-table kernels on the context's stream (no synchronisation, no host copies).
+xatu_status xatu_tables_enqueue(xatu_ctx* ctx) {
   const int na = ctx->natoms;
   const PotParams pp = pot_params(ctx);
-  std::vector<int2> pairs;
-  for (int a = 0; a < na; a++)
-    for (int b = a; b < na; b++) pairs.push_back(make_int2(a, b));
-  const int npairs = (int)pairs.size();
+  const int npairs = na * (na + 1) / 2;
   const int ncells = (int)(ctx->cells.size() / 3);
-  XATU_CK(upload(ctx->d_pairs, pairs.data(), pairs.size(), ctx->stream));
   XATU_CK(ctx->d_VX.ensure((size_t)na * na * sizeof(cd)));
   XATU_CK(cudaMemsetAsync(ctx->d_VX.p, 0, (size_t)na * na * sizeof(cd), ctx->stream));
-  XATU_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
   if (ctx->mode == XATU_MODE_REALSPACE) {
     XATU_CK(ctx->d_vtab.ensure((size_t)npairs * ncells * sizeof(double)));
     XATU_CK(ctx->d_table.ensure((size_t)ctx->nmesh * na * na * sizeof(cd)));
@@ -456,14 +485,14 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
                                                          ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
                                                          ctx->d_vtab.as<double>());
     ctx->launches++;
-    XATU_CK(cudaGetLastError());
+    XATU_CK_LAUNCH("pair_potential_kernel");
     dim3 g2(ctx->nmesh, (npairs + 7) / 8);
     motif_ft_kernel<<<g2, 256, 0, ctx->stream>>>(ctx->nmesh, ctx->d_mesh.as<double>(), ncells,
                                                  ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
                                                  ctx->d_vtab.as<double>(), 1.0 / ctx->total_cells, na,
                                                  ctx->d_table.as<cd>());
     ctx->launches++;
-    XATU_CK(cudaGetLastError());
+    XATU_CK_LAUNCH("motif_ft_kernel");
     if (ctx->exchange) {
       const double* vt = ctx->d_vtab.as<double>();
       if (ctx->exchange_potential != ctx->potential) {
@@ -476,10 +505,8 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
         XATU_CK(cudaGetLastError());
         vt = ctx->d_vtabX.as<double>();
       }
-      XATU_CK(ctx->d_work.ensure(3 * sizeof(double)));
-      XATU_CK(cudaMemcpyAsync(ctx->d_work.p, ctx->Q, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
       dim3 g3(1, (npairs + 7) / 8);
-      motif_ft_kernel<<<g3, 256, 0, ctx->stream>>>(1, ctx->d_work.as<double>(), ncells, ctx->d_cells.as<double>(),
+      motif_ft_kernel<<<g3, 256, 0, ctx->stream>>>(1, ctx->d_Q.as<double>(), ncells, ctx->d_cells.as<double>(),
                                                    npairs, ctx->d_pairs.as<int2>(), vt, 1.0 / ctx->total_cells, na,
                                                    ctx->d_VX.as<cd>());
       ctx->launches++;
@@ -502,6 +529,16 @@ xatu_status xatu_interaction_build(xatu_ctx* ctx) {
       XATU_CK(cudaGetLastError());
     }
   }
+  return XATU_OK;
+}
+
+xatu_status xatu_interaction_build(xatu_ctx* ctx) {
+  if (!ctx) return XATU_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
+  XATU_CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+  xatu_status st = xatu_tables_enqueue(ctx);
+  if (st != XATU_OK) return st;
   XATU_CK(cudaEventRecord(ctx->ev[3], ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   cudaEventElapsedTime(&ctx->stage_ms[1], ctx->ev[2], ctx->ev[3]);
@@ -562,6 +599,53 @@ xatu_status xatu_bse_build_basis(xatu_ctx* ctx, int precision, int64_t nbasis, c
   return build_impl(ctx, precision, ctx->d_basis.as<int>());
 }
 
+void xatu_assembly_setup(const xatu_ctx* ctx, const int* basis, AsmParams* pp, AsmInputs* inp, AsmOutputs* outp) {
+  AsmParams& p = *pp;
+  AsmInputs& in = *inp;
+  AsmOutputs& out = *outp;
+  const int na = ctx->natoms;
+  memset(&p, 0, sizeof(p));
+  p.nk = ctx->nk;
+  p.nv = ctx->nv;
+  p.nc = ctx->nc;
+  p.nb = ctx->nb;
+  p.norb = ctx->norb;
+  p.na = na;
+  p.N = ctx->N;
+  p.mode = ctx->mode;
+  p.exchange = ctx->exchange;
+  p.scissor = ctx->scissor;
+  p.emap.ndim = ctx->ndim;
+  p.emap.n = ctx->n_eff;
+  for (int i = 0; i < 3 * ctx->ndim; i++) p.emap.B[i] = ctx->recip[i];
+  for (int i = 0; i < ctx->ndim * ctx->ndim; i++) p.emap.inv[i] = ctx->inv_gram[i];
+  p.rt_ndim = ctx->ndim;
+  for (int a = 0; a < 3; a++) {
+    p.rt_len[a] = ctx->rt_len[a];
+    p.rt_span[a] = ctx->rt_span[a];
+  }
+  for (int a = 0; a <= na; a++) p.orb_off[a] = ctx->orb_off[a];
+  p.nentries = ctx->mode == XATU_MODE_REALSPACE ? ctx->nmesh : ctx->rt_entries;
+  p.ldk = ctx->ldk;
+  memset(&in, 0, sizeof(in));
+  in.kpoints = ctx->d_kpoints.as<double>();
+  in.kgrid = ctx->d_kgrid.as<int>();
+  in.eigval = ctx->d_eigval.as<double>();
+  in.eigvalQ = ctx->d_eigvalQ.as<double>();
+  in.eigvec = ctx->d_eigvec.as<cd>();
+  in.eigvecQ = ctx->d_eigvecQ.as<cd>();
+  in.table = ctx->d_table.as<cd>();
+  in.exL = ctx->d_exL.as<cd>();
+  in.exR = ctx->d_exR.as<cd>();
+  in.status = ctx->d_status.as<int>();
+  in.basis = basis;
+  memset(&out, 0, sizeof(out));
+  out.H = ctx->d_H.as<cd>();
+  out.Khi = ctx->d_Khi.as<__nv_bfloat162>();
+  out.Klo = ctx->d_Klo.as<__nv_bfloat162>();
+  out.diag = ctx->d_diag.as<double>();
+}
+
 static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis) {
   if (!ctx->has_exciton) return xatu_fail(ctx, XATU_ERR_STATE, "exciton parameters must be set first");
   if (precision != XATU_PREC_FP64 && precision != XATU_PREC_MIXED)
@@ -584,46 +668,9 @@ static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis) {
     XATU_CK(ctx->d_H.ensure((size_t)N * N * sizeof(cd)));
   }
   AsmParams p;
-  memset(&p, 0, sizeof(p));
-  p.nk = ctx->nk;
-  p.nv = ctx->nv;
-  p.nc = ctx->nc;
-  p.nb = ctx->nb;
-  p.norb = ctx->norb;
-  p.na = na;
-  p.N = N;
-  p.mode = ctx->mode;
-  p.exchange = ctx->exchange;
-  p.scissor = ctx->scissor;
-  p.emap.ndim = ctx->ndim;
-  p.emap.n = ctx->n_eff;
-  for (int i = 0; i < 3 * ctx->ndim; i++) p.emap.B[i] = ctx->recip[i];
-  for (int i = 0; i < ctx->ndim * ctx->ndim; i++) p.emap.inv[i] = ctx->inv_gram[i];
-  p.rt_ndim = ctx->ndim;
-  for (int a = 0; a < 3; a++) {
-    p.rt_len[a] = ctx->rt_len[a];
-    p.rt_span[a] = ctx->rt_span[a];
-  }
-  for (int a = 0; a <= na; a++) p.orb_off[a] = ctx->orb_off[a];
-  p.nentries = ctx->mode == XATU_MODE_REALSPACE ? ctx->nmesh : ctx->rt_entries;
-  p.ldk = ctx->ldk;
   AsmInputs in;
-  in.kpoints = ctx->d_kpoints.as<double>();
-  in.kgrid = ctx->d_kgrid.as<int>();
-  in.eigval = ctx->d_eigval.as<double>();
-  in.eigvalQ = ctx->d_eigvalQ.as<double>();
-  in.eigvec = ctx->d_eigvec.as<cd>();
-  in.eigvecQ = ctx->d_eigvecQ.as<cd>();
-  in.table = ctx->d_table.as<cd>();
-  in.exL = ctx->d_exL.as<cd>();
-  in.exR = ctx->d_exR.as<cd>();
-  in.status = ctx->d_status.as<int>();
-  in.basis = basis;
   AsmOutputs out;
-  out.H = ctx->d_H.as<cd>();
-  out.Khi = ctx->d_Khi.as<__nv_bfloat162>();
-  out.Klo = ctx->d_Klo.as<__nv_bfloat162>();
-  out.diag = ctx->d_diag.as<double>();
+  xatu_assembly_setup(ctx, basis, &p, &in, &out);
   XATU_CK(cudaEventRecord(ctx->ev[4], ctx->stream));
   if (ctx->exchange) {
     const int blocks = (int)((N + 127) / 128);
@@ -800,6 +847,14 @@ xatu_status xatu_kernel_stats(const xatu_ctx* ctx, int which, int64_t* launches,
     *launches = ctx->hx_calls;
     *total_ms = ctx->hx_ms;
     *path = ctx->hx_last_path;
+  } else if (which == 2) {
+    *launches = ctx->adjoint_ms > 0 ? 1 : 0;
+    *total_ms = ctx->adjoint_ms;
+    *path = 0;
+  } else if (which == 3) {
+    *launches = ctx->adj_pair_ms > 0 ? 1 : 0;
+    *total_ms = ctx->adj_pair_ms;
+    *path = 0;
   } else {
     return XATU_ERR_INVALID;
   }

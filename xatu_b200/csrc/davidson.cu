@@ -471,7 +471,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   const size_t eigh_smem_max = (size_t)DAV_MAX_BASIS * (DAV_MAX_BASIS + 1) * sizeof(cd) +
                                (DAV_MAX_BASIS / 2 + 2) * sizeof(JacobiRot) + 64 * sizeof(double) +
                                (DAV_MAX_BASIS + 1) * sizeof(int);
-  XATU_CK(cudaFuncSetAttribute(dav_small_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)eigh_smem_max));
+  XATU_CK(xatu_raise_smem_limit((const void*)dav_small_eigh_kernel, eigh_smem_max));
 
   // The basis V (and W = H V) is kept in Ritz form: after every Rayleigh-Ritz
   // step V <- V Y, W <- W Y and T <- diag(theta), so the projected matrix of

@@ -71,7 +71,7 @@ struct xatu_ctx {
   bool kgrid_ok = false;
   int rt_len[3] = {1, 1, 1}, rt_span[3] = {0, 0, 0};
   long long rt_entries = 1;
-  DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid, d_basis;
+  DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid, d_basis, d_Q;
 
   // ---------------- derived device data
   bool bands_ok = false, tables_ok = false;
@@ -97,10 +97,24 @@ struct xatu_ctx {
 
   // ---------------- adjoint
   bool bands_from_model = false;   // bands came from xatu_bands_compute (not uploaded)
-  float adjoint_ms = 0;
+  float adjoint_ms = 0;            // last xatu_adjoint call, first to last launch
+  float adj_pair_ms = 0;           // its pair kernel
   DBuf d_adjX, d_adjdvtab, d_adjdtable, d_adjdVX, d_adjAlpha, d_adjExUW, d_adjCbar, d_adjEbar, d_adjEpart, d_adjGk,
       d_adjG;
 };
+
+// Stage helpers without host synchronisation (api.cu); the batch records them into CUDA graphs.
+extern "C" {
+xatu_status xatu_bands_enqueue(xatu_ctx* ctx);
+xatu_status xatu_tables_enqueue(xatu_ctx* ctx);
+void xatu_assembly_setup(const xatu_ctx* ctx, const int* basis, struct AsmParams* p, struct AsmInputs* in,
+                         struct AsmOutputs* out);
+}
+
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.  The limit is a
+// per-kernel, process-wide setting: lowering it for a small launch would invalidate larger launches of
+// the same kernel already recorded in CUDA graphs or issued by other contexts.
+cudaError_t xatu_raise_smem_limit(const void* kernel, size_t bytes);
 
 // status helpers
 xatu_status xatu_fail(xatu_ctx* ctx, xatu_status code, const std::string& msg);
@@ -122,12 +136,20 @@ xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double*
 cudaError_t xatu_launch_hx_cuda_core(const __nv_bfloat162* Khi, const __nv_bfloat162* Klo, long long ldk, const float2* X,
                                      float2* Y, long long N, int b, cudaStream_t s);
 // tcgen05 version (hx_tc.cu): Bt operands (ng x ldb bf16, hi/lo), Y column-major N x ng FP32.
+// active: NULL, or a device word read by the kernel; 0 skips the product (Y is still zeroed).
 cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, long long ldk, const void* Bhi,
                               const void* Blo, long long ldb, int ng, float* Y, int* status, int num_sms,
-                              cudaStream_t s);
+                              cudaStream_t s, const int* active = nullptr);
 size_t xatu_hx_tc_smem(int ng);
 // W[:, col0 : col0 + nv] = H V[:, col0 : col0 + nv] with the current build (davidson.cu).
 xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv);
+
+// After a kernel launch: the launch's own error, labelled with the kernel.
+#define XATU_CK_LAUNCH(name)                                                       \
+  do {                                                                             \
+    cudaError_t e__ = cudaGetLastError();                                          \
+    if (e__ != cudaSuccess) return xatu_cuda_fail(ctx, e__, "launch of " name);     \
+  } while (0)
 
 #define XATU_CK(call)                                              \
   do {                                                             \

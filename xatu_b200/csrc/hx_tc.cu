@@ -41,6 +41,7 @@ struct HxTcParams {
   int ng;             // 2b, multiple of 16, <= 64
   int nrows;          // N
   int* status;        // device error word
+  const int* active;  // NULL, or a device word: 0 = skip this product (a converged system of a batch)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -136,6 +137,8 @@ hx_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_const
   const uint32_t stage_bytes = 2 * a_bytes + 2 * ((b_bytes + 1023) & ~1023u);
   HxTcSmem* sh = reinterpret_cast<HxTcSmem*>(ring + XHX_STAGES * stage_bytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // the same word for every thread of the grid, read before any barrier or TMEM allocation
+  if (p.active && *p.active == 0) return;
 
   // this CTA's tile range
   const long long t0 = (p.tiles * blockIdx.x) / gridDim.x;
@@ -321,7 +324,7 @@ size_t xatu_hx_tc_smem(int ng) {
 // Y: column-major N x ng FP32, zeroed here.
 cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, long long ldk, const void* Bhi,
                               const void* Blo, long long ldb, int ng, float* Y, int* status, int num_sms,
-                              cudaStream_t s) {
+                              cudaStream_t s, const int* active) {
   if (ng % 16 != 0 || ng < 16 || ng > 64 || (ldk % 4) != 0 || (ldb % 8) != 0) return cudaErrorInvalidValue;
   CUtensorMap ahi, alo, bhi, blo;
   const uint64_t kdim = 2ull * N;
@@ -335,13 +338,14 @@ cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, lon
   p.ng = ng;
   p.nrows = (int)N;
   p.status = status;
+  p.active = active;
   int grid = (int)std::min<long long>(num_sms, p.tiles);
   // a CTA's range must not span more than XHX_NACC m-blocks
   while (grid < p.tiles && (p.tiles + grid - 1) / grid > (long long)(XHX_NACC - 1) * p.ktiles) grid++;
   cudaError_t e = cudaMemsetAsync(Y, 0, sizeof(float) * (size_t)N * ng, s);
   if (e != cudaSuccess) return e;
   const size_t smem = xatu_hx_tc_smem(ng);
-  e = cudaFuncSetAttribute(hx_tcgen05_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = xatu_raise_smem_limit((const void*)hx_tcgen05_kernel, smem);
   if (e != cudaSuccess) return e;
   hx_tcgen05_kernel<<<grid, XHX_THREADS, smem, s>>>(ahi, alo, bhi, blo, p, Y);
   return cudaGetLastError();

@@ -17,3 +17,10 @@ extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoint
 extern "C" size_t band_solve_smem(int norb, int nR, int has_overlap);
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path);
+
+// Batched persistent assembly (assembly.cu), mixed precision, one band-window class per launch.
+bool xatu_assembly_batch_supported(int nv, int nc, int na);
+size_t xatu_assembly_batch_smem(int nv, int nc, int na, int tk, int norb, int exchange);
+cudaError_t xatu_launch_assembly_batch(int nv, int nc, int na, int tk, const AsmBatchMember* members,
+                                       const int2* work, int nwork, int* counter, size_t smem, int num_sms,
+                                       bool set_attr, cudaStream_t s);

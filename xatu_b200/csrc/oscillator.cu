@@ -163,7 +163,7 @@ extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, cons
   XATU_CK(ctx->dv_tmp.ensure(xbytes + 64 * (size_t)nstates));
   XATU_CK(ctx->dv_small.ensure((size_t)3 * nstates * sizeof(cd)));
   const size_t smem = (2 * (size_t)p.norb * p.norb + p.nR + (size_t)p.nb * p.norb) * sizeof(cd) + p.nb * sizeof(double);
-  XATU_CK(cudaFuncSetAttribute(vme_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  XATU_CK(xatu_raise_smem_limit((const void*)vme_kernel, smem));
   vme_kernel<<<ctx->nk, 256, smem, ctx->stream>>>(p, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(),
                                                   ctx->d_HR.as<cd>(), ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr,
                                                   ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),

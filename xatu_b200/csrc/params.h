@@ -3,6 +3,9 @@
 #pragma once
 #include "common.cuh"
 
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current device (api.cu).
+cudaError_t xatu_raise_smem_limit(const void* kernel, size_t bytes);
+
 // Reciprocal-space kernel table: entry e is the k - k' difference with
 // integer grid offsets (e / stride_d) % len_d - span_d along each reciprocal
 // axis, q = q0 + sum_d off_d b_d / n_eff.
@@ -63,6 +66,15 @@ struct AsmOutputs {
   __nv_bfloat162* Khi;     // MIXED: N x N
   __nv_bfloat162* Klo;
   double* diag;            // MIXED: N
+};
+
+// One system of a batched (mixed-precision) assembly launch.
+struct AsmBatchMember {
+  AsmParams p;
+  AsmInputs in;
+  AsmOutputs out;
+  int nblk;                // k blocks of the tile size in use
+  int pad;
 };
 
 

@@ -230,10 +230,9 @@ class ExcitonTB:
         return self.system.nk * len(self.valenceBands) * len(self.conductionBands)
 
     # ------------------------------------------------------------ hot path
-    def initializeHamiltonian(self):
-        """ExcitonTB::initializeHamiltonian (ExcitonTB.cpp:794-815): uploads the
-        system and parameters, then runs the band solve and interaction tables on
-        the device."""
+    def descriptors(self):
+        """(system descriptor, exciton descriptor, kept arrays) of the ABI for this exciton: the
+        checks and defaults of ExcitonTB::initializeHamiltonian (ExcitonTB.cpp:794-815)."""
         s = self.system
         if len(self.valenceBands) + len(self.conductionBands) == 0:
             raise ValueError("Error: Exciton object must have some bands")
@@ -252,7 +251,6 @@ class ExcitonTB:
         sd = L.SystemDesc(s.ndim, L.ptr(keep["brav"]), s.natoms, L.ptr(keep["motif"]), len(keep["orb"]),
                           L.ptr(keep["orb"]), keep["cells"].shape[0], L.ptr(keep["cells"]), L.ptr(keep["ham"]),
                           L.ptr(keep["ovl"]), s.filling, -1, 0)
-        self._call("xatu_system_upload", ctypes.byref(sd))
         keep["kp"] = np.ascontiguousarray(s.kpoints, dtype=np.float64)
         keep["mesh"] = np.ascontiguousarray(s.meshBZ, dtype=np.float64)
         keep["vb"] = np.ascontiguousarray(self.valenceBands, dtype=np.int32)
@@ -265,6 +263,14 @@ class ExcitonTB:
                            L.MODE_REALSPACE if self.mode == "realspace" else L.MODE_RECIPROCAL,
                            self.nReciprocalVectors, pot[self.potential], pot[self.exchangePotential],
                            L.GAUGE_LATTICE if self.gauge == "lattice" else L.GAUGE_ATOMIC)
+        return sd, ed, keep
+
+    def initializeHamiltonian(self):
+        """ExcitonTB::initializeHamiltonian (ExcitonTB.cpp:794-815): uploads the
+        system and parameters, then runs the band solve and interaction tables on
+        the device."""
+        sd, ed, keep = self.descriptors()
+        self._call("xatu_system_upload", ctypes.byref(sd))
         self._call("xatu_exciton_set", ctypes.byref(ed))
         self._call("xatu_bands_compute")
         self._call("xatu_interaction_build")
@@ -406,11 +412,12 @@ class ExcitonTB:
         return {"bands": ms[0], "tables": ms[1], "assembly": ms[2], "solve": ms[3]}
 
     def kernelStats(self, which: str):
-        """(launches, total device ms, path) of "assembly" or "hx" (path 1 CUDA cores, 2 tcgen05)."""
+        """(launches, total device ms, path) of "assembly", "hx" (path 1 CUDA cores, 2 tcgen05), "adjoint"
+        (the last adjoint call) or "adjoint_pair" (its pair kernel)."""
         n = ctypes.c_int64()
         ms = ctypes.c_double()
         path = ctypes.c_int()
-        self._call("xatu_kernel_stats", {"assembly": 0, "hx": 1}[which], ctypes.byref(n), ctypes.byref(ms),
+        self._call("xatu_kernel_stats", {"assembly": 0, "hx": 1, "adjoint": 2, "adjoint_pair": 3}[which], ctypes.byref(n), ctypes.byref(ms),
                    ctypes.byref(path))
         return n.value, ms.value, path.value
 

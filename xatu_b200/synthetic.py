@@ -123,3 +123,34 @@ def random_honeycomb(seed: int, norb_total: int) -> SyntheticConfiguration:
     info.bravaisVectors = cells
     info.norbitals = np.array([n0, n1], dtype=np.int64)
     return SyntheticConfiguration(info, seed, f"random honeycomb {n0}+{n1} orbitals, seed={seed}")
+
+
+def batch_workload(seed: int = 4242, count: int = 64):
+    """The batched workload: ``count`` seeded random honeycomb models of 2-12 orbitals, k grids
+    n x n with n drawn from {24, 36, 48, 60}, 1-3 valence and 1-3 conduction bands (as many as the
+    model has on each side), r0 ~ U(5, 50) Angstrom, eps_s ~ U(1, 6), eps_m = 1, real-space Keldysh,
+    direct term.  Returns a list of dicts (config, ncell, nv, nc, params)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        norb = int(rng.integers(2, 13))
+        cfg = random_honeycomb(seed * 1000 + i, norb)
+        n0 = int(cfg.systemInfo.filling)
+        n1 = int(cfg.systemInfo.norbitals.sum()) - n0
+        ncell = int(rng.choice([24, 36, 48, 60]))
+        nv = int(rng.integers(1, min(3, n0) + 1))
+        nc = int(rng.integers(1, min(3, n1) + 1))
+        r0 = float(rng.uniform(5.0, 50.0))
+        eps_s = float(rng.uniform(1.0, 6.0))
+        out.append({"config": cfg, "ncell": ncell, "nv": nv, "nc": nc, "params": (1.0, eps_s, r0)})
+    return out
+
+
+def exciton_from_spec(spec, device: int = 0):
+    """ExcitonTB of one batch_workload entry (mesh set, nothing on the device yet)."""
+    from .exciton import ExcitonTB
+    nv, nc = spec["nv"], spec["nc"]
+    bands = list(range(-(nv - 1), 1)) + list(range(1, nc + 1))
+    ex = ExcitonTB(spec["config"], spec["ncell"], 1, 0, spec["params"], bands=bands, device=device)
+    ex.brillouinZoneMesh(spec["ncell"])
+    return ex
