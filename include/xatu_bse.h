@@ -202,6 +202,14 @@ xatu_status xatu_oscillator_strength(xatu_ctx *ctx, int nstates, const double *e
 xatu_status xatu_adjoint(xatu_ctx *ctx, int nstates, const double *eigvec, double *grad_hamiltonian,
                          double *grad_params);
 
+/* Summed oscillator strength F = sum_{n: e_lo <= E_n <= e_hi} sum_j |vme_ex_j(n)|^2 of the excitons in an
+   energy window (ResultTB::excitonOscillatorStrength, ResultTB.cpp:242-298, summed over the window) and its
+   gradient dF/d(r0, eps_m, eps_s) through the eigenvectors.  Needs an FP64 build; computes all eigenpairs on
+   the device (dense solver).  *nwindow = number of states in the window; grad_params (3 doubles) may be NULL.
+   No reference counterpart for the gradient. */
+xatu_status xatu_oscillator_window_gradient(xatu_ctx *ctx, double e_lo, double e_hi, int *nwindow, double *F,
+                                            double *grad_params);
+
 /* ------------------------------------------------------------------ batches of systems */
 /* Many BSE instances of uneven size (k grids, band windows, dielectric parameters) built and solved together
    on one GPU.  No reference counterpart (the reference handles one ExcitonTB at a time); each member follows

@@ -30,7 +30,7 @@ EXPORTED_SYMBOLS = [
     "xatu_interaction_build", "xatu_motif_ft_download", "xatu_bse_build", "xatu_bse_dim", "xatu_bse_copy_to_host",
     "xatu_bse_device_buffers", "xatu_bse_solve", "xatu_davidson_config", "xatu_davidson_stats", "xatu_stage_times",
     "xatu_hx_backend", "xatu_kernel_matvec", "xatu_kernel_stats", "xatu_hx_noalloc", "xatu_oscillator_strength",
-    "xatu_bse_build_basis", "xatu_adjoint", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
+    "xatu_bse_build_basis", "xatu_adjoint", "xatu_oscillator_window_gradient", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
     "xatu_batch_set_stream", "xatu_batch_add", "xatu_batch_run", "xatu_batch_dim", "xatu_batch_result",
     "xatu_batch_stats",
     "xatu_kernel_launches", "xatu_reciprocal_lattice", "xatu_mesh_mp", "xatu_mesh_reduced",
@@ -103,6 +103,7 @@ def lib() -> ctypes.CDLL:
         "xatu_oscillator_strength": ([vp, ci, vp, vp], ci),
         "xatu_bse_build_basis": ([vp, ci, ctypes.c_int64, vp], ci),
         "xatu_adjoint": ([vp, ci, vp, vp, vp], ci),
+        "xatu_oscillator_window_gradient": ([vp, ctypes.c_double, ctypes.c_double, vp, vp, vp], ci),
         "xatu_batch_create": ([vp, ci], ci),
         "xatu_batch_destroy": ([vp], ci),
         "xatu_batch_last_error": ([vp], ctypes.c_char_p),

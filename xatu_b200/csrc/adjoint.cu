@@ -590,6 +590,112 @@ static cudaError_t launch_pair_any(const AdjParams& p, const AdjInputs& in, cons
   return cudaErrorInvalidValue;
 }
 
+__global__ void adj_scale_copy_kernel(const cd* __restrict__ in, cd* __restrict__ out, long long n, double f) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+    out[t] = f * in[t];
+}
+
+// Derivative interaction tables into d_adjdtable / d_adjdVX (layouts of d_table / d_VX):
+//   which = 0: d/dr0 (pair potentials or keldyshFT in derivative mode, then the same transforms);
+//   which = 1: d/deps_m = d/deps_s = -V / (2 eps_bar) for the Keldysh potential and its Fourier
+//              transform (scaled copies of the built tables), 0 for the Coulomb potential.
+xatu_status xatu_derivative_tables(xatu_ctx* ctx, int which) {
+  cudaStream_t st = ctx->stream;
+  const int na = ctx->natoms;
+  const int npairs = na * (na + 1) / 2;
+  const int ncells = (int)(ctx->cells.size() / 3);
+  const long long nentries = ctx->mode == XATU_MODE_REALSPACE ? (long long)ctx->nmesh : ctx->rt_entries;
+  XATU_CK(ctx->d_adjdtable.ensure((size_t)nentries * na * na * sizeof(cd)));
+  XATU_CK(ctx->d_adjdVX.ensure((size_t)na * na * sizeof(cd)));
+  XATU_CK(cudaMemsetAsync(ctx->d_adjdVX.p, 0, (size_t)na * na * sizeof(cd), st));
+  if (which == 1) {
+    const double eps_bar = (ctx->eps_m + ctx->eps_s) / 2;
+    const bool dkel = ctx->mode != XATU_MODE_REALSPACE || ctx->potential == XATU_POT_KELDYSH;
+    const bool xkel = ctx->mode != XATU_MODE_REALSPACE || ctx->exchange_potential == XATU_POT_KELDYSH;
+    const long long n = nentries * na * na;
+    adj_scale_copy_kernel<<<(int)std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(
+        ctx->d_table.as<cd>(), ctx->d_adjdtable.as<cd>(), n, dkel ? -1.0 / (2 * eps_bar) : 0.0);
+    ctx->launches++;
+    XATU_CK_LAUNCH("adj_scale_copy_kernel");
+    if (ctx->exchange) {
+      adj_scale_copy_kernel<<<1, 256, 0, st>>>(ctx->d_VX.as<cd>(), ctx->d_adjdVX.as<cd>(), (long long)na * na,
+                                               xkel ? -1.0 / (2 * eps_bar) : 0.0);
+      ctx->launches++;
+      XATU_CK_LAUNCH("adj_scale_copy_kernel");
+    }
+    return XATU_OK;
+  }
+  PotParams pp;
+  pp.a1norm = ctx->a1;
+  pp.b1norm = ctx->b1;
+  pp.area = ctx->area;
+  pp.eps_m = ctx->eps_m;
+  pp.eps_s = ctx->eps_s;
+  pp.r0 = ctx->r0;
+  pp.regularization = ctx->regularization;
+  pp.cutoff = ctx->cutoff;
+  pp.total_cells = ctx->total_cells;
+  if (ctx->mode == XATU_MODE_REALSPACE) {
+    XATU_CK(ctx->d_adjdvtab.ensure((size_t)npairs * ncells * sizeof(double)));
+    const long long tot = (long long)npairs * ncells;
+    const int grid = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
+    pair_potential_kernel<<<grid, 256, 0, st>>>(pp, ctx->potential, 1, na, ctx->d_motif.as<double>(), ncells,
+                                                ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
+                                                ctx->d_adjdvtab.as<double>());
+    ctx->launches++;
+    XATU_CK_LAUNCH("pair_potential_kernel (d/dr0)");
+    dim3 g2(ctx->nmesh, (npairs + 7) / 8);
+    motif_ft_kernel<<<g2, 256, 0, st>>>(ctx->nmesh, ctx->d_mesh.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
+                                        ctx->d_pairs.as<int2>(), ctx->d_adjdvtab.as<double>(), 1.0 / ctx->total_cells,
+                                        na, ctx->d_adjdtable.as<cd>());
+    ctx->launches++;
+    XATU_CK_LAUNCH("motif_ft_kernel (d/dr0)");
+    if (ctx->exchange) {
+      pair_potential_kernel<<<grid, 256, 0, st>>>(pp, ctx->exchange_potential, 1, na, ctx->d_motif.as<double>(),
+                                                  ncells, ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
+                                                  ctx->d_adjdvtab.as<double>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("pair_potential_kernel (exchange, d/dr0)");
+      dim3 g3(1, (npairs + 7) / 8);
+      motif_ft_kernel<<<g3, 256, 0, st>>>(1, ctx->d_Q.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
+                                          ctx->d_pairs.as<int2>(), ctx->d_adjdvtab.as<double>(),
+                                          1.0 / ctx->total_cells, na, ctx->d_adjdVX.as<cd>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("motif_ft_kernel (exchange, d/dr0)");
+    }
+  } else {
+    RecipTable t;
+    memset(&t, 0, sizeof(t));
+    t.ndim = ctx->ndim;
+    t.n_eff = ctx->n_eff;
+    for (int a = 0; a < 3; a++) {
+      t.span[a] = ctx->rt_span[a];
+      t.len[a] = ctx->rt_len[a];
+    }
+    for (int i = 0; i < 3 * ctx->ndim; i++) t.b[i] = ctx->recip[i];
+    t.nG = (int)(ctx->G.size() / 3);
+    const long long tot = nentries * na;
+    const int grid = (int)std::min<long long>((tot + 127) / 128, 148 * 32);
+    recip_table_kernel<<<grid, 128, 0, st>>>(pp, t, 1, (int)nentries, ctx->d_G.as<double>(), na,
+                                             ctx->d_motif.as<double>(), ctx->d_adjdtable.as<cd>());
+    ctx->launches++;
+    XATU_CK_LAUNCH("recip_table_kernel (d/dr0)");
+    if (ctx->exchange) {
+      RecipTable tx = t;
+      for (int a = 0; a < 3; a++) {
+        tx.span[a] = 0;
+        tx.len[a] = 1;
+        tx.q0[a] = ctx->Q[a];
+      }
+      recip_table_kernel<<<1, 128, 0, st>>>(pp, tx, 1, 1, ctx->d_G.as<double>(), na, ctx->d_motif.as<double>(),
+                                            ctx->d_adjdVX.as<cd>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("recip_table_kernel (exchange, d/dr0)");
+    }
+  }
+  return XATU_OK;
+}
+
 extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* eigvec, double* grad_hamiltonian,
                                     double* grad_params) {
   if (!ctx || !eigvec || nstates < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
@@ -612,84 +718,11 @@ extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* ei
   // eigenvectors, derivative tables
   XATU_CK(ctx->d_adjX.ensure((size_t)N * ns * sizeof(cd)));
   XATU_CK(cudaMemcpyAsync(ctx->d_adjX.p, eigvec, (size_t)N * ns * sizeof(cd), cudaMemcpyHostToDevice, st));
-  PotParams pp;
-  pp.a1norm = ctx->a1;
-  pp.b1norm = ctx->b1;
-  pp.area = ctx->area;
-  pp.eps_m = ctx->eps_m;
-  pp.eps_s = ctx->eps_s;
-  pp.r0 = ctx->r0;
-  pp.regularization = ctx->regularization;
-  pp.cutoff = ctx->cutoff;
-  pp.total_cells = ctx->total_cells;
-  const int npairs = na * (na + 1) / 2;
-  const int ncells = (int)(ctx->cells.size() / 3);
-  XATU_CK(ctx->d_adjdVX.ensure((size_t)na * na * sizeof(cd)));
-  XATU_CK(cudaMemsetAsync(ctx->d_adjdVX.p, 0, (size_t)na * na * sizeof(cd), st));
-  long long nentries;
-  if (ctx->mode == XATU_MODE_REALSPACE) {
-    nentries = ctx->nmesh;
-    XATU_CK(ctx->d_adjdvtab.ensure((size_t)npairs * ncells * sizeof(double)));
-    XATU_CK(ctx->d_adjdtable.ensure((size_t)nentries * na * na * sizeof(cd)));
-    const long long tot = (long long)npairs * ncells;
-    const int grid = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
-    pair_potential_kernel<<<grid, 256, 0, st>>>(pp, ctx->potential, 1, na, ctx->d_motif.as<double>(), ncells,
-                                                ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
-                                                ctx->d_adjdvtab.as<double>());
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
-    dim3 g2(ctx->nmesh, (npairs + 7) / 8);
-    motif_ft_kernel<<<g2, 256, 0, st>>>(ctx->nmesh, ctx->d_mesh.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
-                                        ctx->d_pairs.as<int2>(), ctx->d_adjdvtab.as<double>(), 1.0 / ctx->total_cells,
-                                        na, ctx->d_adjdtable.as<cd>());
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
-    if (ctx->exchange) {
-      pair_potential_kernel<<<grid, 256, 0, st>>>(pp, ctx->exchange_potential, 1, na, ctx->d_motif.as<double>(),
-                                                  ncells, ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
-                                                  ctx->d_adjdvtab.as<double>());
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-      dim3 g3(1, (npairs + 7) / 8);
-      motif_ft_kernel<<<g3, 256, 0, st>>>(1, ctx->d_Q.as<double>(), ncells, ctx->d_cells.as<double>(), npairs,
-                                          ctx->d_pairs.as<int2>(), ctx->d_adjdvtab.as<double>(),
-                                          1.0 / ctx->total_cells, na, ctx->d_adjdVX.as<cd>());
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-    }
-  } else {
-    nentries = ctx->rt_entries;
-    RecipTable t;
-    memset(&t, 0, sizeof(t));
-    t.ndim = ctx->ndim;
-    t.n_eff = ctx->n_eff;
-    for (int a = 0; a < 3; a++) {
-      t.span[a] = ctx->rt_span[a];
-      t.len[a] = ctx->rt_len[a];
-    }
-    for (int i = 0; i < 3 * ctx->ndim; i++) t.b[i] = ctx->recip[i];
-    t.nG = (int)(ctx->G.size() / 3);
-    XATU_CK(ctx->d_adjdtable.ensure((size_t)nentries * na * na * sizeof(cd)));
-    const long long tot = nentries * na;
-    const int grid = (int)std::min<long long>((tot + 127) / 128, 148 * 32);
-    recip_table_kernel<<<grid, 128, 0, st>>>(pp, t, 1, (int)nentries, ctx->d_G.as<double>(), na,
-                                             ctx->d_motif.as<double>(), ctx->d_adjdtable.as<cd>());
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
-    if (ctx->exchange) {
-      RecipTable tx = t;
-      for (int a = 0; a < 3; a++) {
-        tx.span[a] = 0;
-        tx.len[a] = 1;
-        tx.q0[a] = ctx->Q[a];
-      }
-      recip_table_kernel<<<1, 128, 0, st>>>(pp, tx, 1, 1, ctx->d_G.as<double>(), na, ctx->d_motif.as<double>(),
-                                            ctx->d_adjdVX.as<cd>());
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-    }
+  {
+    xatu_status s0 = xatu_derivative_tables(ctx, 0);
+    if (s0 != XATU_OK) return s0;
   }
-
+  const long long nentries = ctx->mode == XATU_MODE_REALSPACE ? (long long)ctx->nmesh : ctx->rt_entries;
   // exchange: alpha, u = VX conj(alpha), w = VX^T alpha (host, na x na)
   std::vector<cd> alpha((size_t)ns * na, mk(0, 0)), VX((size_t)na * na, mk(0, 0)), dVX((size_t)na * na, mk(0, 0));
   std::vector<cd> exu((size_t)ns * na), exw((size_t)ns * na);

@@ -15,7 +15,9 @@ __global__ void conj_columns_kernel(cd* v, long long n) {
     v[t].y = -v[t].y;
 }
 
-xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec) {
+// All eigenpairs of the FP64 build on the device: eigenvalues ascending in dv_diagH, eigenvectors as the
+// columns of dv_V (column-major N x N; conjugated back when `vectors`).
+xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors) {
   const long long N = ctx->N;
   if (!ctx->solver) {
     if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS)
@@ -32,7 +34,7 @@ xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double*
   if (cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS)
     return xatu_fail(ctx, XATU_ERR_CUDA, "cusolverDnCreateParams failed");
   size_t dev_ws = 0, host_ws = 0;
-  const cusolverEigMode_t jobz = eigvec ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+  const cusolverEigMode_t jobz = vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
   cusolverStatus_t cs = cusolverDnXsyevd_bufferSize(ctx->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, N, CUDA_C_64F,
                                                      ctx->dv_V.p, N, CUDA_R_64F, ctx->dv_diagH.p, CUDA_C_64F, &dev_ws,
                                                      &host_ws);
@@ -55,14 +57,22 @@ xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double*
   XATU_CK(cudaMemcpyAsync(&info, ctx->dv_small.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   if (info != 0) return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "cusolverDnXsyevd reported info != 0");
-  const long long ns = (nstates <= 0) ? N : nstates;
-  XATU_CK(cudaMemcpyAsync(eigval, ctx->dv_diagH.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  if (eigvec) {
-    conj_columns_kernel<<<592, 256, 0, ctx->stream>>>(ctx->dv_V.as<cd>(), ns * N);
+  if (vectors) {
+    conj_columns_kernel<<<592, 256, 0, ctx->stream>>>(ctx->dv_V.as<cd>(), N * N);
     ctx->launches++;
     XATU_CK(cudaGetLastError());
-    XATU_CK(cudaMemcpyAsync(eigvec, ctx->dv_V.p, (size_t)ns * N * sizeof(cd), cudaMemcpyDeviceToHost, ctx->stream));
   }
+  return XATU_OK;
+}
+
+xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec) {
+  const long long N = ctx->N;
+  xatu_status st = xatu_dense_eig_device(ctx, eigvec != nullptr);
+  if (st != XATU_OK) return st;
+  const long long ns = (nstates <= 0) ? N : nstates;
+  XATU_CK(cudaMemcpyAsync(eigval, ctx->dv_diagH.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (eigvec)
+    XATU_CK(cudaMemcpyAsync(eigvec, ctx->dv_V.p, (size_t)ns * N * sizeof(cd), cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   return XATU_OK;
 }

@@ -131,6 +131,13 @@ struct AsmOutputs;
 xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec);
 // Dense FP64 (dense.cu): all eigenpairs with cuSOLVER.
 xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double* eigvec);
+// The same, left on the device: eigenvalues in dv_diagH, eigenvectors as columns of dv_V (N x N).
+xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors);
+// Velocity matrix elements of every e-h state into out (3 x N, row-major) (oscillator.cu).
+xatu_status xatu_vme_enqueue(xatu_ctx* ctx, cd* out);
+// Derivative interaction tables (adjoint.cu): which = 0: d/dr0, 1: d/deps_m (= d/deps_s), into
+// d_adjdtable (same layout as d_table) and d_adjdVX (as d_VX).
+xatu_status xatu_derivative_tables(xatu_ctx* ctx, int which);
 
 // K.X products (hx.cu).  Y[N x b] = (Khi + Klo) X, all row-major complex float.
 cudaError_t xatu_launch_hx_cuda_core(const __nv_bfloat162* Khi, const __nv_bfloat162* Klo, long long ldk, const float2* X,

@@ -13,6 +13,8 @@
 // for n = conduction, n' = valence; the element the exciton sum uses is
 // vme(v, c) = conj(vme(c, v)).
 // exciton_vme_kernel: vme_ex(j, s) = sum_i X_is v_j(i), one CTA per (j, s).
+#include <cstring>
+
 #include "engine.h"
 
 #define OSC_BOHR 0.52917721067121
@@ -136,14 +138,8 @@ extern "C" __global__ void exciton_vme_kernel(const cd* __restrict__ v, const cd
   }
 }
 
-extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, const double* eigvec, double* vme_ex) {
-  if (!ctx || !eigvec || !vme_ex || nstates < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
-  cudaSetDevice(ctx->device);
-  if (!ctx->bands_ok) return xatu_fail(ctx, XATU_ERR_STATE, "bands are not computed");
-  if (ctx->custom_basis)
-    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "oscillator strengths need the full e-h basis (last build used a subset)");
-  if (nstates > ctx->N) return xatu_fail(ctx, XATU_ERR_INVALID, "nstates larger than the BSE dimension");
-  const long long N = ctx->N;
+// Velocity matrix elements of every e-h state of the full basis into out (3 x N, row-major).
+xatu_status xatu_vme_enqueue(xatu_ctx* ctx, cd* out) {
   OscParams p;
   memset(&p, 0, sizeof(p));
   p.nk = ctx->nk;
@@ -157,19 +153,31 @@ extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, cons
   for (int a = 0; a <= ctx->natoms; a++) p.orb_off[a] = ctx->orb_off[a];
   for (int a = 0; a < ctx->natoms; a++)
     for (int d = 0; d < 3; d++) p.pos[3 * a + d] = ctx->motif[4 * a + d];
+  const size_t smem = (2 * (size_t)p.norb * p.norb + p.nR + (size_t)p.nb * p.norb) * sizeof(cd) + p.nb * sizeof(double);
+  XATU_CK(xatu_raise_smem_limit((const void*)vme_kernel, smem));
+  vme_kernel<<<ctx->nk, 256, smem, ctx->stream>>>(p, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(),
+                                                  ctx->d_HR.as<cd>(), ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr,
+                                                  ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(), out);
+  ctx->launches++;
+  XATU_CK_LAUNCH("vme_kernel");
+  return XATU_OK;
+}
+
+extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, const double* eigvec, double* vme_ex) {
+  if (!ctx || !eigvec || !vme_ex || nstates < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
+  cudaSetDevice(ctx->device);
+  if (!ctx->bands_ok) return xatu_fail(ctx, XATU_ERR_STATE, "bands are not computed");
+  if (ctx->custom_basis)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "oscillator strengths need the full e-h basis (last build used a subset)");
+  if (nstates > ctx->N) return xatu_fail(ctx, XATU_ERR_INVALID, "nstates larger than the BSE dimension");
+  const long long N = ctx->N;
   const size_t vbytes = (size_t)3 * N * sizeof(cd);
   const size_t xbytes = (size_t)N * nstates * sizeof(cd);
   XATU_CK(ctx->dv_R.ensure(vbytes));
   XATU_CK(ctx->dv_tmp.ensure(xbytes + 64 * (size_t)nstates));
   XATU_CK(ctx->dv_small.ensure((size_t)3 * nstates * sizeof(cd)));
-  const size_t smem = (2 * (size_t)p.norb * p.norb + p.nR + (size_t)p.nb * p.norb) * sizeof(cd) + p.nb * sizeof(double);
-  XATU_CK(xatu_raise_smem_limit((const void*)vme_kernel, smem));
-  vme_kernel<<<ctx->nk, 256, smem, ctx->stream>>>(p, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(),
-                                                  ctx->d_HR.as<cd>(), ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr,
-                                                  ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
-                                                  ctx->dv_R.as<cd>());
-  ctx->launches++;
-  XATU_CK(cudaGetLastError());
+  xatu_status st = xatu_vme_enqueue(ctx, ctx->dv_R.as<cd>());
+  if (st != XATU_OK) return st;
   XATU_CK(cudaMemcpyAsync(ctx->dv_tmp.p, eigvec, xbytes, cudaMemcpyHostToDevice, ctx->stream));
   exciton_vme_kernel<<<3 * nstates, 256, 0, ctx->stream>>>(ctx->dv_R.as<cd>(), ctx->dv_tmp.as<cd>(), (int)N, nstates,
                                                            ctx->dv_small.as<cd>());

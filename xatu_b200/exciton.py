@@ -383,6 +383,19 @@ class ExcitonTB:
             out["r0"], out["eps_m"], out["eps_s"] = P[:, 0].copy(), P[:, 1].copy(), P[:, 2].copy()
         return out
 
+    def oscillatorWindowGradient(self, e_lo: float, e_hi: float, gradient: bool = True) -> dict:
+        """Summed oscillator strength F of the excitons with e_lo <= E <= e_hi (FP64 build needed) and
+        dF/dr0, dF/deps_m, dF/deps_s through the eigenvectors: {"F", "nwindow", "r0", "eps_m", "eps_s"}."""
+        nw = ctypes.c_int()
+        F = ctypes.c_double()
+        g = np.zeros(3)
+        self._call("xatu_oscillator_window_gradient", float(e_lo), float(e_hi), ctypes.byref(nw), ctypes.byref(F),
+                   L.ptr(g) if gradient else None)
+        out = {"F": F.value, "nwindow": nw.value}
+        if gradient:
+            out["r0"], out["eps_m"], out["eps_s"] = float(g[0]), float(g[1]), float(g[2])
+        return out
+
     def davidsonConfig(self, tol: float = 0.0, max_iter: int = 0, block: int = 0):
         self._call("xatu_davidson_config", float(tol), int(max_iter), int(block))
 
