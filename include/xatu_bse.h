@@ -204,11 +204,13 @@ xatu_status xatu_adjoint(xatu_ctx *ctx, int nstates, const double *eigvec, doubl
 
 /* Summed oscillator strength F = sum_{n: e_lo <= E_n <= e_hi} sum_j |vme_ex_j(n)|^2 of the excitons in an
    energy window (ResultTB::excitonOscillatorStrength, ResultTB.cpp:242-298, summed over the window) and its
-   gradient dF/d(r0, eps_m, eps_s) through the eigenvectors.  Needs an FP64 build; computes all eigenpairs on
-   the device (dense solver).  *nwindow = number of states in the window; grad_params (3 doubles) may be NULL.
-   No reference counterpart for the gradient. */
+   gradients: dF/d(r0, eps_m, eps_s) through the eigenvectors (grad_params, 3 doubles) and dF/dH(R)
+   (grad_hamiltonian, nR x norb x norb complex, same convention as xatu_adjoint) through the eigenvectors, the
+   bands and the velocity matrix elements; either may be NULL.  Needs an FP64 build; computes all eigenpairs
+   on the device (dense solver).  *nwindow = number of states in the window.  The hopping gradient needs bands
+   from the model, Q = 0 and full (non-triangular) storage.  No reference counterpart for the gradient. */
 xatu_status xatu_oscillator_window_gradient(xatu_ctx *ctx, double e_lo, double e_hi, int *nwindow, double *F,
-                                            double *grad_params);
+                                            double *grad_params, double *grad_hamiltonian);
 
 /* ------------------------------------------------------------------ batches of systems */
 /* Many BSE instances of uneven size (k grids, band windows, dielectric parameters) built and solved together

@@ -52,3 +52,36 @@ def test_oscillator_window_value_and_gradient(case):
         assert nwp == nw and nwm == nw
         fd = (Fp - Fm) / (2 * h)
         assert abs(g[name] - fd) <= 1e-5 * max(abs(fd), 1e-6 * F0), (name, g[name], fd)
+
+
+def _oracle_F_hr(case, lo, hi, HR):
+    ex = oracle_case(case, HR=HR)
+    w, X = np.linalg.eigh(ex.H)
+    sel = (w >= lo) & (w <= hi)
+    v = exciton_oscillator_strength(ex, X[:, sel])
+    return float(np.sum(np.abs(v) ** 2)), int(sel.sum())
+
+
+@pytest.mark.parametrize("case", ["hbn_real", "hbn_recip_exch", "syn_real_exch"])
+def test_oscillator_window_hopping_gradient(case):
+    """dF/dH(R) through the eigenvectors, the bands and the velocity matrix elements, against central
+    differences of the oracle along Hermitian-consistent hopping directions."""
+    from grad_cases import PICKS, hopping_directions
+    ex = engine_case(case)
+    ex.BShamiltonian("fp64")
+    E = ex.diagonalize("diag", 1).eigval
+    lo, hi = _window(np.sort(E))
+    g = ex.oscillatorWindowGradient(lo, hi, gradient=False, hamiltonian=True)
+    HR = ex.system.hamiltonianMatrices.copy()
+    cells = ex.system.unitCellList
+    ex.close()
+    G = g["hamiltonian"]
+    scale = np.abs(G).max()
+    h = 1e-6
+    for d in hopping_directions(HR, cells, PICKS):
+        Fp, nwp = _oracle_F_hr(case, lo, hi, HR + h * d)
+        Fm, nwm = _oracle_F_hr(case, lo, hi, HR - h * d)
+        assert nwp == g["nwindow"] and nwm == g["nwindow"]
+        fd = (Fp - Fm) / (2 * h)
+        pred = float(np.real(np.sum(np.conj(G) * d)))
+        assert abs(pred - fd) <= 1e-5 * scale, (pred, fd, scale)

@@ -103,7 +103,7 @@ def lib() -> ctypes.CDLL:
         "xatu_oscillator_strength": ([vp, ci, vp, vp], ci),
         "xatu_bse_build_basis": ([vp, ci, ctypes.c_int64, vp], ci),
         "xatu_adjoint": ([vp, ci, vp, vp, vp], ci),
-        "xatu_oscillator_window_gradient": ([vp, ctypes.c_double, ctypes.c_double, vp, vp, vp], ci),
+        "xatu_oscillator_window_gradient": ([vp, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp], ci),
         "xatu_batch_create": ([vp, ci], ci),
         "xatu_batch_destroy": ([vp], ci),
         "xatu_batch_last_error": ([vp], ctypes.c_char_p),

@@ -696,6 +696,333 @@ xatu_status xatu_derivative_tables(xatu_ctx* ctx, int which) {
   return XATU_OK;
 }
 
+// cbar / ebar (ns x nk x nb x norb, ns x nk x nb) -> G(R) in d_adjG (ns x nR x norb x norb): the band
+// eigensystems are recomputed and the adjoint pulled back through fixGlobalPhase and the eigenproblem.
+xatu_status xatu_adjoint_bands_to_hoppings(xatu_ctx* ctx, int ns, const cd* cbar, const double* ebar) {
+  cudaStream_t st = ctx->stream;
+  const int nk = ctx->nk, norb = ctx->norb, nb = ctx->nb;
+  BandParams bp;
+  memset(&bp, 0, sizeof(bp));
+  bp.nk = nk;
+  bp.norb = norb;
+  bp.nR = ctx->nR;
+  bp.triangular = ctx->triangular;
+  bp.nb = nb;
+  for (int i = 0; i < nb; i++) bp.band_list[i] = ctx->band_list[i];
+  bp.max_sweeps = 40;
+  bp.has_overlap = ctx->has_overlap ? 1 : 0;
+  bp.is_au = ctx->is_au ? 1 : 0;
+  const size_t n2 = (size_t)norb * norb;
+  XATU_CK(ctx->d_adjGk.ensure((ctx->qnonzero ? 2 : 1) * (size_t)ns * nk * n2 * sizeof(cd)));
+  const cd* SR = ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr;
+  cd* g0 = ctx->d_adjGk.as<cd>();
+  cd* gQ = ctx->qnonzero ? g0 + (size_t)ns * nk * n2 : nullptr;
+  const int r1 = ctx->qnonzero ? ctx->nv : nb;
+  const size_t smem = adj_band_smem(norb, ctx->nR, bp.has_overlap, r1);
+  const size_t smemQ = ctx->qnonzero ? adj_band_smem(norb, ctx->nR, bp.has_overlap, nb - ctx->nv) : 0;
+  if (std::max(smem, smemQ) > 227 * 1024)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "adjoint band kernel: orbital basis too large for shared memory");
+  XATU_CK(xatu_raise_smem_limit((const void*)adj_band_kernel, std::max(smem, smemQ)));
+  adj_band_kernel<<<nk, ADJ_BAND_THREADS, smem, st>>>(bp, ns, 0, r1, ctx->d_kpoints.as<double>(),
+                                                      ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR, cbar, ebar, g0,
+                                                      ctx->d_status.as<int>());
+  ctx->launches++;
+  XATU_CK_LAUNCH("adj_band_kernel");
+  if (ctx->qnonzero) {
+    for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
+    adj_band_kernel<<<nk, ADJ_BAND_THREADS, smemQ, st>>>(bp, ns, ctx->nv, nb, ctx->d_kpoints.as<double>(),
+                                                        ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR, cbar,
+                                                        ebar, gQ, ctx->d_status.as<int>());
+    ctx->launches++;
+    XATU_CK_LAUNCH("adj_band_kernel (k+Q)");
+  }
+  XATU_CK(ctx->d_adjG.ensure((size_t)ns * ctx->nR * n2 * sizeof(cd)));
+  dim3 gh(ctx->nR, (unsigned)((n2 + 255) / 256), ns);
+  adj_hop_kernel<<<gh, 256, 0, st>>>(nk, norb, ctx->triangular ? 1 : 0, ctx->d_kpoints.as<double>(),
+                                     ctx->d_cellsR.as<double>(), g0, gQ, ctx->Q[0], ctx->Q[1], ctx->Q[2],
+                                     ctx->d_adjG.as<cd>(), ctx->nR);
+  ctx->launches++;
+  XATU_CK_LAUNCH("adj_hop_kernel");
+  return XATU_OK;
+}
+
+// ------------------------------------------------------------------ weight-matrix form
+// The same back-propagation for a general Hermitian weight matrix Y (row-major N x N): the derivative of
+// sum_ij Y_ij H_ij, i.e. of sum_t 2 Re(a_t^H H b_t) when Y = sum_t (conj(a_t) b_t^T + conj(b_t) a_t^T).
+// Exchange factors: Zc = Y conj(L), Zv = Y^T L (N x na, column-major) with the exchange vectors L.
+struct AdjWeightInputs {
+  const cd* Y;        // row-major N x N
+  const cd* Zc;       // N x na, or NULL without exchange
+  const cd* Zv;
+  const cd* VX;       // na x na
+};
+
+template <int NV, int NC, int NA>
+__global__ void __launch_bounds__(ADJ_THREADS) adj_pair_weight_kernel(AdjParams p, AdjInputs in, AdjWeightInputs wi,
+                                                                       cd* __restrict__ cbar, double* __restrict__ ebar) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NB = NV + NC, NCV = NC * NV;
+  constexpr int WC = NC * NA * NC;
+  const int norb = p.norb, k = blockIdx.x, tid = threadIdx.x;
+  cd* Ck = reinterpret_cast<cd*>(smem_raw);    // NB x norb
+  cd* acc = Ck + NB * norb;                    // NB x norb
+  cd* w = acc + NB * norb;                     // (WC + NV NA NV) x ADJ_THREADS
+  __shared__ int atom_of[XATU_MAX_ORB];
+  for (int t = tid; t < NB * norb; t += ADJ_THREADS) {
+    const int b = t / norb;
+    Ck[t] = (b < NV ? in.eigvec : in.eigvecQ)[(int64_t)k * p.nb * norb + t];
+    acc[t] = mk(0, 0);
+  }
+  for (int o = tid; o < norb; o += ADJ_THREADS) {
+    int a = 0;
+    while (a + 1 < NA && o >= p.orb_off[a + 1]) a++;
+    atom_of[o] = a;
+  }
+  __syncthreads();
+  for (int base = 0; base < p.nk; base += ADJ_THREADS) {
+    const int k2 = base + tid;
+    const int nq = min(ADJ_THREADS, p.nk - base);
+    if (k2 < p.nk) {
+      cd P[NA][NC][NC], R[NA][NV][NV];
+      const cd* c2 = in.eigvec + (int64_t)k2 * p.nb * norb;
+      const cd* c2q = in.eigvecQ + (int64_t)k2 * p.nb * norb;
+#pragma unroll
+      for (int a = 0; a < NA; a++) {
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+#pragma unroll
+          for (int c2i = 0; c2i < NC; c2i++) P[a][c][c2i] = mk(0, 0);
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+          for (int v2 = 0; v2 < NV; v2++) R[a][v][v2] = mk(0, 0);
+        for (int o = p.orb_off[a]; o < p.orb_off[a + 1]; o++) {
+          cd cq[NC], vv[NV];
+#pragma unroll
+          for (int c2i = 0; c2i < NC; c2i++) cq[c2i] = c2q[(NV + c2i) * norb + o];
+#pragma unroll
+          for (int v2 = 0; v2 < NV; v2++) vv[v2] = c2[v2 * norb + o];
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            const cd ck = Ck[(NV + c) * norb + o];
+#pragma unroll
+            for (int c2i = 0; c2i < NC; c2i++) P[a][c][c2i] = P[a][c][c2i] + cmulc(ck, cq[c2i]);
+          }
+#pragma unroll
+          for (int v = 0; v < NV; v++) {
+            const cd vk = Ck[v * norb + o];
+#pragma unroll
+            for (int v2 = 0; v2 < NV; v2++) R[a][v2][v] = R[a][v2][v] + cmulc(vv[v2], vk);
+          }
+        }
+      }
+      int64_t e = interaction_entry(p, in.kpoints, in.kgrid, k, k2);
+      if (e < 0) {
+        atomicOr(in.status, XATU_DEVERR_INDEX);
+        e = 0;
+      }
+      const cd* Vt = in.table + e * NA * NA;
+      cd Yb[NCV][NCV];
+#pragma unroll
+      for (int r = 0; r < NCV; r++)
+#pragma unroll
+        for (int c = 0; c < NCV; c++) Yb[r][c] = wi.Y[((int64_t)k * NCV + r) * p.N + (int64_t)k2 * NCV + c];
+      cd* wt = w + tid;
+      // wc[c][a][c'] = -sum_{v,v'} Y[cv][c'v'] sum_b V_ab R_b(v', v)
+#pragma unroll
+      for (int a = 0; a < NA; a++) {
+        cd VR[NV][NV];
+#pragma unroll
+        for (int v2 = 0; v2 < NV; v2++)
+#pragma unroll
+          for (int v = 0; v < NV; v++) {
+            cd t = mk(0, 0);
+#pragma unroll
+            for (int b = 0; b < NA; b++) t = t + Vt[a * NA + b] * R[b][v2][v];
+            VR[v2][v] = t;
+          }
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+#pragma unroll
+          for (int c2i = 0; c2i < NC; c2i++) {
+            cd t = mk(0, 0);
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+#pragma unroll
+              for (int v2 = 0; v2 < NV; v2++) t = t + Yb[c * NV + v][c2i * NV + v2] * VR[v2][v];
+            wt[((c * NA + a) * NC + c2i) * ADJ_THREADS] = mk(-t.x, -t.y);
+          }
+      }
+      // wv[v][b][v'] = -sum_{c,c'} conj(Y[cv][c'v']) conj(sum_a P_a(c, c') V_ab)
+#pragma unroll
+      for (int b = 0; b < NA; b++) {
+        cd PV[NC][NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+#pragma unroll
+          for (int c2i = 0; c2i < NC; c2i++) {
+            cd t = mk(0, 0);
+#pragma unroll
+            for (int a = 0; a < NA; a++) t = t + P[a][c][c2i] * Vt[a * NA + b];
+            PV[c][c2i] = t;
+          }
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+          for (int v2 = 0; v2 < NV; v2++) {
+            cd t = mk(0, 0);
+#pragma unroll
+            for (int c = 0; c < NC; c++)
+#pragma unroll
+              for (int c2i = 0; c2i < NC; c2i++) t = t + Yb[c * NV + v][c2i * NV + v2] * PV[c][c2i];
+            wt[(WC + (v * NA + b) * NV + v2) * ADJ_THREADS] = mk(-t.x, t.y);   // -conj(t)
+          }
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < NB * norb; t += ADJ_THREADS) {
+      const int b = t / norb, o = t - b * norb, a = atom_of[o];
+      cd sum = mk(0, 0);
+      if (b >= NV) {
+        const int c = b - NV;
+        for (int q = 0; q < nq; q++) {
+          const cd* ww = w + (c * NA + a) * NC * ADJ_THREADS + q;
+          const cd* cq = in.eigvecQ + ((int64_t)(base + q) * p.nb + NV) * norb + o;
+#pragma unroll
+          for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_THREADS] * cq[c2i * norb];
+        }
+      } else {
+        for (int q = 0; q < nq; q++) {
+          const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_THREADS + q;
+          const cd* cv = in.eigvec + (int64_t)(base + q) * p.nb * norb + o;
+#pragma unroll
+          for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_THREADS] * cv[v2 * norb];
+        }
+      }
+      acc[t] = acc[t] + sum;
+    }
+    __syncthreads();
+  }
+  // exchange (per state i of row k: u(i) = VX Zc(i), w(i) = VX^T Zv(i)) and outputs
+  for (int t = tid; t < NB * norb; t += ADJ_THREADS) {
+    const int b = t / norb, o = t - b * norb, a = atom_of[o];
+    cd v = acc[t];
+    if (wi.Zc) {
+      if (b >= NV) {
+        const int c = b - NV;
+        for (int vv = 0; vv < NV; vv++) {
+          const int64_t i = (int64_t)k * NCV + c * NV + vv;
+          cd u = mk(0, 0);
+          for (int b2 = 0; b2 < NA; b2++) u = u + wi.VX[a * NA + b2] * wi.Zc[(int64_t)b2 * p.N + i];
+          v = v + Ck[vv * norb + o] * u;
+        }
+      } else {
+        for (int c = 0; c < NC; c++) {
+          const int64_t i = (int64_t)k * NCV + c * NV + b;
+          cd u = mk(0, 0);
+          for (int a2 = 0; a2 < NA; a2++) u = u + wi.VX[a2 * NA + a] * wi.Zv[(int64_t)a2 * p.N + i];
+          v = v + Ck[(NV + c) * norb + o] * u;
+        }
+      }
+    }
+    cbar[((int64_t)k * NB + b) * norb + o] = v;
+  }
+  for (int b = tid; b < NB; b += ADJ_THREADS) {
+    double e = 0.0;
+    if (b >= NV) {
+      for (int vv = 0; vv < NV; vv++) {
+        const int64_t i = (int64_t)k * NCV + (b - NV) * NV + vv;
+        e += wi.Y[i * p.N + i].x;
+      }
+    } else {
+      for (int c = 0; c < NC; c++) {
+        const int64_t i = (int64_t)k * NCV + c * NV + b;
+        e -= wi.Y[i * p.N + i].x;
+      }
+    }
+    ebar[(int64_t)k * NB + b] = e;
+  }
+}
+
+template <int NV, int NC, int NA>
+static cudaError_t launch_weight(const AdjParams& p, const AdjInputs& in, const AdjWeightInputs& wi, cd* cbar,
+                                 double* ebar, cudaStream_t st) {
+  const int nb = NV + NC;
+  const int wn = NC * NA * NC + NV * NA * NV;
+  const size_t smem = ((size_t)2 * nb * p.norb + (size_t)ADJ_THREADS * wn) * sizeof(cd);
+  cudaError_t e = xatu_raise_smem_limit((const void*)adj_pair_weight_kernel<NV, NC, NA>, smem);
+  if (e != cudaSuccess) return e;
+  adj_pair_weight_kernel<NV, NC, NA><<<p.nk, ADJ_THREADS, smem, st>>>(p, in, wi, cbar, ebar);
+  return cudaGetLastError();
+}
+
+template <int NV, int NC>
+static cudaError_t launch_weight_na(const AdjParams& p, const AdjInputs& in, const AdjWeightInputs& wi, cd* cbar,
+                                    double* ebar, cudaStream_t st) {
+  switch (p.na) {
+    case 1: return launch_weight<NV, NC, 1>(p, in, wi, cbar, ebar, st);
+    case 2: return launch_weight<NV, NC, 2>(p, in, wi, cbar, ebar, st);
+    case 3: return launch_weight<NV, NC, 3>(p, in, wi, cbar, ebar, st);
+    case 4: return launch_weight<NV, NC, 4>(p, in, wi, cbar, ebar, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+static AdjParams adj_params(const xatu_ctx* ctx, int ns) {
+  AdjParams p;
+  memset(&p, 0, sizeof(p));
+  p.nk = ctx->nk;
+  p.nv = ctx->nv;
+  p.nc = ctx->nc;
+  p.nb = ctx->nb;
+  p.norb = ctx->norb;
+  p.na = ctx->natoms;
+  p.ns = ns;
+  p.N = ctx->N_full;
+  p.mode = ctx->mode == XATU_MODE_REALSPACE ? 0 : 1;
+  p.emap.ndim = ctx->ndim;
+  p.emap.n = ctx->n_eff;
+  for (int i = 0; i < 3 * ctx->ndim; i++) p.emap.B[i] = ctx->recip[i];
+  for (int i = 0; i < ctx->ndim * ctx->ndim; i++) p.emap.inv[i] = ctx->inv_gram[i];
+  p.rt_ndim = ctx->ndim;
+  for (int a = 0; a < 3; a++) {
+    p.rt_len[a] = ctx->rt_len[a];
+    p.rt_span[a] = ctx->rt_span[a];
+  }
+  p.nentries = ctx->mode == XATU_MODE_REALSPACE ? (long long)ctx->nmesh : ctx->rt_entries;
+  for (int a = 0; a <= ctx->natoms; a++) p.orb_off[a] = ctx->orb_off[a];
+  return p;
+}
+
+// Weighted back-propagation through the assembly: cbar (nk x nb x norb), ebar (nk x nb) of
+// sum_ij Y_ij H_ij for the row-major weight matrix Y on the device.
+xatu_status xatu_adjoint_weighted(xatu_ctx* ctx, const cd* Y, const cd* Zc, const cd* Zv, cd* cbar, double* ebar) {
+  if (ctx->nv > 2 || ctx->nc > 2 || ctx->natoms > 4)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "adjoint supports at most 2 valence, 2 conduction bands and 4 atoms");
+  const AdjParams p = adj_params(ctx, 1);
+  AdjInputs in;
+  memset(&in, 0, sizeof(in));
+  in.kpoints = ctx->d_kpoints.as<double>();
+  in.kgrid = ctx->d_kgrid.as<int>();
+  in.eigvec = ctx->d_eigvec.as<cd>();
+  in.eigvecQ = ctx->d_eigvecQ.as<cd>();
+  in.table = ctx->d_table.as<cd>();
+  in.status = ctx->d_status.as<int>();
+  AdjWeightInputs wi;
+  wi.Y = Y;
+  wi.Zc = Zc;
+  wi.Zv = Zv;
+  wi.VX = ctx->d_VX.as<cd>();
+  cudaError_t e = cudaErrorInvalidValue;
+  if (p.nv == 1 && p.nc == 1) e = launch_weight_na<1, 1>(p, in, wi, cbar, ebar, ctx->stream);
+  if (p.nv == 1 && p.nc == 2) e = launch_weight_na<1, 2>(p, in, wi, cbar, ebar, ctx->stream);
+  if (p.nv == 2 && p.nc == 1) e = launch_weight_na<2, 1>(p, in, wi, cbar, ebar, ctx->stream);
+  if (p.nv == 2 && p.nc == 2) e = launch_weight_na<2, 2>(p, in, wi, cbar, ebar, ctx->stream);
+  ctx->launches++;
+  XATU_CK(e);
+  return XATU_OK;
+}
+
 extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* eigvec, double* grad_hamiltonian,
                                     double* grad_params) {
   if (!ctx || !eigvec || nstates < 1) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
@@ -840,48 +1167,9 @@ extern "C" xatu_status xatu_adjoint(xatu_ctx* ctx, int nstates, const double* ei
 
   // hopping matrices
   if (grad_hamiltonian) {
-    BandParams bp;
-    memset(&bp, 0, sizeof(bp));
-    bp.nk = nk;
-    bp.norb = norb;
-    bp.nR = ctx->nR;
-    bp.triangular = ctx->triangular;
-    bp.nb = nb;
-    for (int i = 0; i < nb; i++) bp.band_list[i] = ctx->band_list[i];
-    bp.max_sweeps = 40;
-    bp.has_overlap = ctx->has_overlap ? 1 : 0;
-    bp.is_au = ctx->is_au ? 1 : 0;
+    xatu_status sb = xatu_adjoint_bands_to_hoppings(ctx, ns, out.cbar, out.ebar);
+    if (sb != XATU_OK) return sb;
     const size_t n2 = (size_t)norb * norb;
-    XATU_CK(ctx->d_adjGk.ensure((ctx->qnonzero ? 2 : 1) * (size_t)ns * nk * n2 * sizeof(cd)));
-    const cd* SR = ctx->has_overlap ? ctx->d_SR.as<cd>() : nullptr;
-    cd* g0 = ctx->d_adjGk.as<cd>();
-    cd* gQ = ctx->qnonzero ? g0 + (size_t)ns * nk * n2 : nullptr;
-    const int r1 = ctx->qnonzero ? ctx->nv : nb;
-    size_t smem = adj_band_smem(norb, ctx->nR, bp.has_overlap, r1);
-    const size_t smemQ = ctx->qnonzero ? adj_band_smem(norb, ctx->nR, bp.has_overlap, nb - ctx->nv) : 0;
-    if (std::max(smem, smemQ) > 227 * 1024)
-      return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "adjoint band kernel: orbital basis too large for shared memory");
-    XATU_CK(xatu_raise_smem_limit((const void*)adj_band_kernel, std::max(smem, smemQ)));
-    adj_band_kernel<<<nk, ADJ_BAND_THREADS, smem, st>>>(bp, ns, 0, r1, ctx->d_kpoints.as<double>(),
-                                                        ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
-                                                        out.cbar, out.ebar, g0, ctx->d_status.as<int>());
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
-    if (ctx->qnonzero) {
-      for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
-      adj_band_kernel<<<nk, ADJ_BAND_THREADS, smemQ, st>>>(bp, ns, ctx->nv, nb, ctx->d_kpoints.as<double>(),
-                                                          ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(), SR,
-                                                          out.cbar, out.ebar, gQ, ctx->d_status.as<int>());
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-    }
-    XATU_CK(ctx->d_adjG.ensure((size_t)ns * ctx->nR * n2 * sizeof(cd)));
-    dim3 gh(ctx->nR, (unsigned)((n2 + 255) / 256), ns);
-    adj_hop_kernel<<<gh, 256, 0, st>>>(nk, norb, ctx->triangular ? 1 : 0, ctx->d_kpoints.as<double>(),
-                                       ctx->d_cellsR.as<double>(), g0, gQ, ctx->Q[0], ctx->Q[1], ctx->Q[2],
-                                       ctx->d_adjG.as<cd>(), ctx->nR);
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
     XATU_CK(cudaMemcpyAsync(grad_hamiltonian, ctx->d_adjG.p, (size_t)ns * ctx->nR * n2 * sizeof(cd),
                             cudaMemcpyDeviceToHost, st));
     XATU_CK(cudaStreamSynchronize(st));

@@ -99,6 +99,7 @@ struct xatu_ctx {
   bool bands_from_model = false;   // bands came from xatu_bands_compute (not uploaded)
   float adjoint_ms = 0;            // last xatu_adjoint call, first to last launch
   float adj_pair_ms = 0;           // its pair kernel
+  DBuf d_oscG;
   DBuf d_adjX, d_adjdvtab, d_adjdtable, d_adjdVX, d_adjAlpha, d_adjExUW, d_adjCbar, d_adjEbar, d_adjEpart, d_adjGk,
       d_adjG;
 };
@@ -135,9 +136,19 @@ xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double*
 xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors);
 // Velocity matrix elements of every e-h state into out (3 x N, row-major) (oscillator.cu).
 xatu_status xatu_vme_enqueue(xatu_ctx* ctx, cd* out);
+// Adjoint of the velocity matrix elements (oscillator.cu): vbar (N x 3, column-major) -> added to cbar/ebar
+// and, for the direct dependence on H(R), to G (nR x norb x norb); gvme: scratch of 2 x nk x norb^2.
+// G = NULL: only cbar/ebar and gvme; xatu_vme_hop_enqueue then adds the direct part to G.
+xatu_status xatu_vme_adjoint_enqueue(xatu_ctx* ctx, const cd* vbar, cd* cbar, double* ebar, cd* gvme, cd* G);
+xatu_status xatu_vme_hop_enqueue(xatu_ctx* ctx, const cd* gvme, cd* G);
 // Derivative interaction tables (adjoint.cu): which = 0: d/dr0, 1: d/deps_m (= d/deps_s), into
 // d_adjdtable (same layout as d_table) and d_adjdVX (as d_VX).
 xatu_status xatu_derivative_tables(xatu_ctx* ctx, int which);
+// Band-level back-propagation (adjoint.cu): cbar/ebar of ns objectives -> G(R) in d_adjG.
+xatu_status xatu_adjoint_bands_to_hoppings(xatu_ctx* ctx, int ns, const cd* cbar, const double* ebar);
+// cbar/ebar of sum_ij Y_ij H_ij for a Hermitian row-major weight matrix Y (adjoint.cu); Zc = Y conj(L),
+// Zv = Y^T L with the exchange vectors L (NULL without exchange).
+xatu_status xatu_adjoint_weighted(xatu_ctx* ctx, const cd* Y, const cd* Zc, const cd* Zv, cd* cbar, double* ebar);
 
 // K.X products (hx.cu).  Y[N x b] = (Khi + Klo) X, all row-major complex float.
 cudaError_t xatu_launch_hx_cuda_core(const __nv_bfloat162* Khi, const __nv_bfloat162* Klo, long long ldk, const float2* X,

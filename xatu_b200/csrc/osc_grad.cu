@@ -46,11 +46,12 @@ __global__ void og_scale_kernel(cd* C, long long N, int n0, int nw, const double
 }
 
 static xatu_status og_zgemm(xatu_ctx* ctx, cublasOperation_t ta, cublasOperation_t tb, long long m, long long n,
-                            long long k, const cd* A, long long lda, const cd* B, long long ldb, cd* C, long long ldc) {
+                            long long k, const cd* A, long long lda, const cd* B, long long ldb, cd* C, long long ldc,
+                            bool accumulate = false) {
   static const cuDoubleComplex one = {1.0, 0.0}, zero = {0.0, 0.0};
   cublasStatus_t s = cublasZgemm(ctx->blas, ta, tb, (int)m, (int)n, (int)k, &one,
                                  reinterpret_cast<const cuDoubleComplex*>(A), (int)lda,
-                                 reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, &zero,
+                                 reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, accumulate ? &one : &zero,
                                  reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
   if (s != CUBLAS_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZgemm failed");
   return XATU_OK;
@@ -94,12 +95,15 @@ static xatu_status og_build_derivative(xatu_ctx* ctx, int which, cd* out) {
 }
 
 extern "C" xatu_status xatu_oscillator_window_gradient(xatu_ctx* ctx, double e_lo, double e_hi, int* nwindow,
-                                                       double* F, double* grad_params) {
+                                                       double* F, double* grad_params, double* grad_hamiltonian) {
   if (!ctx || !F) return xatu_fail(ctx, XATU_ERR_INVALID, "bad argument");
   cudaSetDevice(ctx->device);
   if (ctx->built_prec != XATU_PREC_FP64) return xatu_fail(ctx, XATU_ERR_STATE, "needs an FP64 build (xatu_bse_build)");
   if (ctx->custom_basis) return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "needs the full e-h basis");
   if (!(e_hi >= e_lo)) return xatu_fail(ctx, XATU_ERR_INVALID, "empty energy window");
+  if (grad_hamiltonian && (!ctx->bands_from_model || ctx->qnonzero || ctx->triangular))
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED,
+                     "hopping gradient of the oscillator strength needs bands from the model, Q = 0 and full storage");
   const long long N = ctx->N;
   cudaStream_t st = ctx->stream;
   if (!ctx->blas) {
@@ -121,6 +125,7 @@ extern "C" xatu_status xatu_oscillator_window_gradient(xatu_ctx* ctx, double e_l
   *F = 0.0;
   if (grad_params)
     for (int q = 0; q < 3; q++) grad_params[q] = 0.0;
+  if (grad_hamiltonian) memset(grad_hamiltonian, 0, 2 * sizeof(double) * (size_t)ctx->nR * ctx->norb * ctx->norb);
   if (nw == 0) return XATU_OK;
   const cd* X = ctx->dv_V.as<cd>();
   const cd* XW = X + (long long)n0 * N;
@@ -140,7 +145,7 @@ extern "C" xatu_status xatu_oscillator_window_gradient(xatu_ctx* ctx, double e_l
   double f = 0.0;
   for (const cd& z : Zh) f += nrm2(z);
   *F = f;
-  if (!grad_params) return XATU_OK;
+  if (!grad_params && !grad_hamiltonian) return XATU_OK;
   // b_n = sum_j vme_ex_j(n) conj(v_j): B = conj(v Z^H)
   OG_TRY(og_zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_C, N, nw, 3, v, N, Z, nw, B, N));
   og_conj_kernel<<<592, 256, 0, st>>>(B, N * nw);
@@ -160,22 +165,74 @@ extern "C" xatu_status xatu_oscillator_window_gradient(xatu_ctx* ctx, double e_l
   // dF/dtheta = 2 Re <lambda, dH X_W> for theta = r0, eps (= eps_m = eps_s)
   XATU_CK(ctx->dv_W.ensure((size_t)N * N * sizeof(cd)));
   cd* dH = ctx->dv_W.as<cd>();
-  for (int which = 0; which < 2; which++) {
-    OG_TRY(og_build_derivative(ctx, which, dH));
-    // G = dH X_W; dH is row-major, i.e. the column-major buffer holds dH^T
-    OG_TRY(og_zgemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, N, nw, N, dH, N, XW, N, C, N));
-    cuDoubleComplex dot;
-    if (cublasZdotc(ctx->blas, (int)(N * nw), reinterpret_cast<const cuDoubleComplex*>(Lam), 1,
-                    reinterpret_cast<const cuDoubleComplex*>(C), 1, &dot) != CUBLAS_STATUS_SUCCESS)
-      return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZdotc failed");
-    const double g = 2.0 * dot.x;
-    if (which == 0) {
-      grad_params[0] = g;
-    } else {
-      grad_params[1] = g;
-      grad_params[2] = g;
+  if (grad_params) {
+    for (int which = 0; which < 2; which++) {
+      OG_TRY(og_build_derivative(ctx, which, dH));
+      // G = dH X_W; dH is row-major, i.e. the column-major buffer holds dH^T
+      OG_TRY(og_zgemm(ctx, CUBLAS_OP_T, CUBLAS_OP_N, N, nw, N, dH, N, XW, N, C, N));
+      cuDoubleComplex dot;
+      if (cublasZdotc(ctx->blas, (int)(N * nw), reinterpret_cast<const cuDoubleComplex*>(Lam), 1,
+                      reinterpret_cast<const cuDoubleComplex*>(C), 1, &dot) != CUBLAS_STATUS_SUCCESS)
+        return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZdotc failed");
+      const double g = 2.0 * dot.x;
+      if (which == 0) {
+        grad_params[0] = g;
+      } else {
+        grad_params[1] = g;
+        grad_params[2] = g;
+      }
     }
+    XATU_CK(cudaStreamSynchronize(st));
+    OG_TRY(xatu_check_device_status(ctx, "oscillator window gradient (derivative assembly)"));
   }
+  if (!grad_hamiltonian) return XATU_OK;
+  // hopping matrices.  (1) through the eigenvectors: dF = sum_ij Y_ij dH_ij with the Hermitian weight
+  // Y = conj(Lambda) X_W^T + conj(X_W) Lambda^T, stored row-major (= the column-major X_W Lambda^H + Lambda X_W^H)
+  cd* Yr = dH;
+  OG_TRY(og_zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_C, N, N, nw, XW, N, Lam, N, Yr, N));
+  OG_TRY(og_zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_C, N, N, nw, Lam, N, XW, N, Yr, N, true));
+  const int na = ctx->natoms, nk = ctx->nk, nb = ctx->nb, norb = ctx->norb;
+  cd* Zc = nullptr;
+  cd* Zv = nullptr;
+  XATU_CK(ctx->dv_tmp.ensure((size_t)2 * N * na * sizeof(cd) + (size_t)N * 3 * sizeof(cd) + 64));
+  if (ctx->exchange) {
+    XATU_CK(ctx->d_exL.ensure((size_t)N * na * sizeof(cd)));
+    XATU_CK(ctx->d_exR.ensure((size_t)N * na * sizeof(cd)));
+    exchange_vectors_kernel<<<(int)((N + 127) / 128), 128, 0, st>>>(
+        (int)N, ctx->nv, ctx->nc, nb, norb, na, ctx->d_orboff.as<int>(), ctx->d_eigvec.as<cd>(), ctx->d_eigvecQ.as<cd>(),
+        ctx->d_VX.as<cd>(), nullptr, ctx->d_exL.as<cd>(), ctx->d_exR.as<cd>());
+    ctx->launches++;
+    XATU_CK_LAUNCH("exchange_vectors_kernel");
+    // L[i * na + a] is the column-major na x N matrix M; Zc = Y M^H = Yt^T M^H, Zv = Y^T M^T = Yt M^T
+    Zc = ctx->dv_tmp.as<cd>();
+    Zv = Zc + (size_t)N * na;
+    OG_TRY(og_zgemm(ctx, CUBLAS_OP_T, CUBLAS_OP_C, N, na, N, Yr, N, ctx->d_exL.as<cd>(), na, Zc, N));
+    OG_TRY(og_zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_T, N, na, N, Yr, N, ctx->d_exL.as<cd>(), na, Zv, N));
+  }
+  XATU_CK(ctx->d_adjCbar.ensure((size_t)nk * nb * norb * sizeof(cd)));
+  XATU_CK(ctx->d_adjEbar.ensure((size_t)nk * nb * sizeof(double)));
+  cd* cbar = ctx->d_adjCbar.as<cd>();
+  double* ebar = ctx->d_adjEbar.as<double>();
+  OG_TRY(xatu_adjoint_weighted(ctx, Yr, Zc, Zv, cbar, ebar));
+  // (2) through the velocity matrix elements: vbar = dF/dconj(v) = conj(X_W conj(Z))
+  cd* vbar = ctx->dv_tmp.as<cd>() + (size_t)2 * N * na;
+  {
+    std::vector<cd> Zcj(Zh.size());
+    for (size_t q = 0; q < Zh.size(); q++) Zcj[q] = conj(Zh[q]);
+    XATU_CK(cudaMemcpyAsync(Z, Zcj.data(), Zcj.size() * sizeof(cd), cudaMemcpyHostToDevice, st));
+    OG_TRY(og_zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, N, 3, nw, XW, N, Z, nw, vbar, N));
+    og_conj_kernel<<<592, 256, 0, st>>>(vbar, N * 3);
+    ctx->launches++;
+    XATU_CK_LAUNCH("og_conj_kernel");
+    XATU_CK(cudaStreamSynchronize(st));   // Zcj leaves scope
+  }
+  XATU_CK(ctx->d_oscG.ensure((size_t)2 * nk * norb * norb * sizeof(cd)));
+  OG_TRY(xatu_vme_adjoint_enqueue(ctx, vbar, cbar, ebar, ctx->d_oscG.as<cd>(), nullptr));
+  // bands -> G(R), then the direct H(R) part of the velocity matrix elements
+  OG_TRY(xatu_adjoint_bands_to_hoppings(ctx, 1, cbar, ebar));
+  OG_TRY(xatu_vme_hop_enqueue(ctx, ctx->d_oscG.as<cd>(), ctx->d_adjG.as<cd>()));
+  XATU_CK(cudaMemcpyAsync(grad_hamiltonian, ctx->d_adjG.p, (size_t)ctx->nR * norb * norb * sizeof(cd),
+                          cudaMemcpyDeviceToHost, st));
   XATU_CK(cudaStreamSynchronize(st));
-  return xatu_check_device_status(ctx, "oscillator window gradient (derivative assembly)");
+  return xatu_check_device_status(ctx, "oscillator window gradient (hopping matrices)");
 }

@@ -383,17 +383,24 @@ class ExcitonTB:
             out["r0"], out["eps_m"], out["eps_s"] = P[:, 0].copy(), P[:, 1].copy(), P[:, 2].copy()
         return out
 
-    def oscillatorWindowGradient(self, e_lo: float, e_hi: float, gradient: bool = True) -> dict:
-        """Summed oscillator strength F of the excitons with e_lo <= E <= e_hi (FP64 build needed) and
-        dF/dr0, dF/deps_m, dF/deps_s through the eigenvectors: {"F", "nwindow", "r0", "eps_m", "eps_s"}."""
+    def oscillatorWindowGradient(self, e_lo: float, e_hi: float, gradient: bool = True,
+                                 hamiltonian: bool = False) -> dict:
+        """Summed oscillator strength F of the excitons with e_lo <= E <= e_hi (FP64 build needed) and its
+        gradients: {"F", "nwindow", "r0", "eps_m", "eps_s"} and, with hamiltonian=True, "hamiltonian"
+        (nR x norb x norb, dF = Re sum conj(G) dH for Hermitian-consistent perturbations)."""
         nw = ctypes.c_int()
         F = ctypes.c_double()
         g = np.zeros(3)
+        s = self.system
+        G = np.zeros((s.hamiltonianMatrices.shape[0], s.basisdim, s.basisdim), dtype=np.complex128) \
+            if hamiltonian else None
         self._call("xatu_oscillator_window_gradient", float(e_lo), float(e_hi), ctypes.byref(nw), ctypes.byref(F),
-                   L.ptr(g) if gradient else None)
+                   L.ptr(g) if gradient else None, L.ptr(G) if G is not None else None)
         out = {"F": F.value, "nwindow": nw.value}
         if gradient:
             out["r0"], out["eps_m"], out["eps_s"] = float(g[0]), float(g[1]), float(g[2])
+        if G is not None:
+            out["hamiltonian"] = G
         return out
 
     def davidsonConfig(self, tol: float = 0.0, max_iter: int = 0, block: int = 0):
