@@ -254,6 +254,49 @@ def adjoint_workload(ncell: int, stream, hbm: float) -> dict:
         worst = max(worst, float(np.max(np.abs(pred - fd) / scale)))
     checks["hopping_directions"] = worst
     ex.system.hamiltonianMatrices = HR
+    # summed oscillator strength in a 0.2 eV window above the lowest state: value and gradients
+    solve()
+    Eall = ex.diagonalize("diag", 1).eigval
+    lo = Eall[0] - 1e-3
+    kk = int(np.searchsorted(Eall, Eall[0] + 0.2, side="right")) - 1
+    while kk + 1 < len(Eall) and Eall[kk + 1] - Eall[kk] < 1e-3:
+        kk += 1
+    hi = 0.5 * (Eall[kk] + Eall[kk + 1])
+    o0 = torch.cuda.Event(enable_timing=True)
+    o1 = torch.cuda.Event(enable_timing=True)
+    o0.record(stream)
+    osc = ex.oscillatorWindowGradient(lo, hi, gradient=True, hamiltonian=True)
+    o1.record(stream)
+    torch.cuda.synchronize()
+    osc_ms = o0.elapsed_time(o1)
+
+    def window_F():
+        ex.initializeHamiltonian()
+        ex.BShamiltonian("fp64")
+        return ex.oscillatorWindowGradient(lo, hi, gradient=False)
+
+    osc_checks = {}
+    hh = h * abs(ex.r0)
+    ex.setParameters([ex.eps_m, ex.eps_s, p0[2] + hh])
+    Fp = window_F()
+    ex.setParameters([ex.eps_m, ex.eps_s, p0[2] - hh])
+    Fm = window_F()
+    ex.setParameters(p0)
+    fd = (Fp["F"] - Fm["F"]) / (2 * hh)
+    osc_checks["r0"] = abs(osc["r0"] - fd) / abs(fd)
+    d = np.zeros_like(HR)
+    rm = int(np.argmin(np.linalg.norm(cells + cells[1], axis=1)))
+    d[1, 0, 9] = 1.0
+    d[rm, 9, 0] = 1.0
+    ex.system.hamiltonianMatrices = HR + h * d
+    Fp = window_F()
+    ex.system.hamiltonianMatrices = HR - h * d
+    Fm = window_F()
+    ex.system.hamiltonianMatrices = HR
+    fd = (Fp["F"] - Fm["F"]) / (2 * h)
+    pred = float(np.real(np.sum(np.conj(osc["hamiltonian"]) * d)))
+    osc_checks["hopping_direction"] = abs(pred - fd) / np.abs(osc["hamiltonian"]).max()
+    osc_checks["window_states_stable"] = bool(Fp["nwindow"] == osc["nwindow"] == Fm["nwindow"])
     nk, norb, na, nv, nc = ncell * ncell, ex.system.basisdim, ex.system.natoms, 2, 2
     # algorithmic flops of the pair kernel (complex multiply-add = 8 flops): per (k, k') pair the factors
     # P, R ((nc^2 + nv^2) norb), per state the contractions with the tables and the state vectors and the
@@ -270,7 +313,12 @@ def adjoint_workload(ncell: int, stream, hbm: float) -> dict:
            "pair_kernel": {"bound": "fp64", "achieved": flops / pair_s / 1e12, "peak": fp64, "unit": "TFLOP/s",
                            "frac": flops / pair_s / 1e12 / fp64, "peak_source": "measured cuBLAS FP64 GEMM "
                            "(torch.matmul float64 4096^3) in this run", "algorithmic_flops": flops},
-           "fd_rel_err": checks, "fd_h": h, "energies_eV": E0.tolist()}
+           "fd_rel_err": checks, "fd_h": h, "energies_eV": E0.tolist(),
+           "oscillator_window": {"window_eV": [float(lo), float(hi)], "states": osc["nwindow"], "F": osc["F"],
+                                 "dF_dr0": osc["r0"], "dF_deps_m": osc["eps_m"], "ms": osc_ms,
+                                 "path": "all eigenpairs (dense FP64), lambda by ZGEMM, dH/dtheta assembled, "
+                                         "weight-matrix adjoint + velocity-matrix-element adjoint for H(R)",
+                                 "fd_rel_err": osc_checks}}
     ex.close()
     return out
 

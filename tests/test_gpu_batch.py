@@ -70,3 +70,33 @@ def test_batch_rejects_unsupported_member():
         batch.run(NST)
     batch.close()
     ex.close()
+
+
+def test_batch_exchange_and_reciprocal_members():
+    """Members with the exchange term and in reciprocal-space mode, next to a plain one."""
+    specs = _specs()[:3]
+    settings = [dict(exchange=True), dict(mode="reciprocalspace", nG=3, exchange=True), dict()]
+
+    def make(spec, opt):
+        ex = exciton_from_spec(spec)
+        ex.setExchange(opt.get("exchange", False))
+        if "mode" in opt:
+            ex.setMode(opt["mode"])
+            ex.setReciprocalVectors(opt["nG"])
+        return ex
+
+    batch = ExcitonBatch()
+    exs = [make(s, o) for s, o in zip(specs, settings)]
+    for ex in exs:
+        batch.add(ex)
+    batch.run(NST)
+    for i, (s, o) in enumerate(zip(specs, settings)):
+        ref = make(s, o)
+        ref.initializeHamiltonian()
+        ref.BShamiltonian("fp64")
+        e_ref = ref.diagonalize("diag", NST).eigval[:NST]
+        ref.close()
+        assert np.abs(batch.result(i)[0] - e_ref).max() < 1e-4, (i, o)
+    batch.close()
+    for ex in exs:
+        ex.close()

@@ -112,13 +112,21 @@ def test_generic_assembly_path_matches(monkeypatch):
     assert rel_err(H2, H1) < 1e-13
 
 
-def test_three_band_window_generic():
-    """nv = nc = 3 runs the generic kernel; parity with the oracle."""
+def test_three_band_window_tiles(monkeypatch):
+    """nv = nc = 3 runs the 8 x 8-tile kernel (FP64 and mixed); parity with the oracle and with the
+    generic kernel, exchange included."""
     cfg = model_config("MoS2.model")
-    ex, orc = _pair(cfg, 5, 3, [1., 4., 13.55])
+    ex, orc = _pair(cfg, 5, 3, [1., 4., 13.55], exchange=True)
     ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
     ex.BShamiltonian("fp64")
-    assert rel_err(ex.HBS, orc.bs_hamiltonian()) < FP64_TOL
+    assert ex.kernelStats("assembly")[2] == 0          # tile path
+    H = ex.HBS
+    assert rel_err(H, orc.bs_hamiltonian()) < FP64_TOL
+    ex.BShamiltonian("mixed")
+    assert rel_err(ex.HBS, H) < MIXED_TOL
+    monkeypatch.setenv("XATU_FORCE_GENERIC_ASSEMBLY", "1")
+    ex.BShamiltonian("fp64")
+    assert rel_err(ex.HBS, H) < 1e-13
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -1,0 +1,52 @@
+// Single-system tile assembly, float: one CTA per upper-triangular (k-block, k'-block) tile
+// (assemble_tile, assembly_tile.cuh).  Tile side 16 k points for windows of up to 4 e-h pairs per k,
+// 8 for larger windows (the staging tile grows with (nv nc)^2).
+#include "assembly_tile.cuh"
+
+template <typename T, int NV, int NC, int NA, bool MIXED, int TK>
+__global__ void __launch_bounds__(TK * TK)
+bse_assemble_tile_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
+  assemble_tile<T, NV, NC, NA, MIXED, TK>(p, in, out, nblk, blockIdx.x);
+}
+
+template <typename T, int NV, int NC, int NA, bool MIXED>
+static cudaError_t launch_tile(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s) {
+  constexpr int TK = (NV * NC <= 4) ? 16 : 8;
+  const int nblk = (p.nk + TK - 1) / TK;
+  const int ntiles = nblk * (nblk + 1) / 2;
+  constexpr int TR = TK * NV * NC;
+  const size_t smem = (2 * (size_t)(NV + NC) * p.norb * TK + (size_t)TR * (TR + 1) +
+                       (p.exchange ? 2 * (size_t)TR * NA : 0)) *
+                      sizeof(cplx<T>);
+  if (smem > 200 * 1024) return cudaErrorNotSupported;
+  auto kern = bse_assemble_tile_kernel<T, NV, NC, NA, MIXED, TK>;
+  cudaError_t e = xatu_raise_smem_limit((const void*)kern, smem);
+  if (e != cudaSuccess) return e;
+  kern<<<ntiles, TK * TK, smem, s>>>(p, in, out, nblk);
+  return cudaGetLastError();
+}
+
+// Launches the tile kernel of the band-window class of p; *launched = false when the class has none.
+cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
+                          bool* launched) {
+  *launched = true;
+#define XATU_CASE(NVv, NCv)                                                                  \
+  if (p.nv == NVv && p.nc == NCv) {                                                          \
+    if (p.na == 1) return launch_tile<float, NVv, NCv, 1, true>(p, in, out, s);                 \
+    if (p.na == 2) return launch_tile<float, NVv, NCv, 2, true>(p, in, out, s);                 \
+    if (p.na == 3) return launch_tile<float, NVv, NCv, 3, true>(p, in, out, s);                 \
+    if (p.na == 4) return launch_tile<float, NVv, NCv, 4, true>(p, in, out, s);                 \
+  }
+  XATU_CASE(1, 1)
+  XATU_CASE(1, 2)
+  XATU_CASE(1, 3)
+  XATU_CASE(2, 1)
+  XATU_CASE(2, 2)
+  XATU_CASE(2, 3)
+  XATU_CASE(3, 1)
+  XATU_CASE(3, 2)
+  XATU_CASE(3, 3)
+#undef XATU_CASE
+  *launched = false;
+  return cudaSuccess;
+}

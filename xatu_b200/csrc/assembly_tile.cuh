@@ -1,0 +1,360 @@
+// BSE matrix assembly (ExcitonTB::BShamiltonian, ExcitonTB.cpp:840-921).
+//
+// For e-h states i = (k, c, v) and j = (k', c', v') (row order of
+// Exciton::createBasis, Exciton.tpp:128-147: i = k*nc*nv + c*nv + v):
+//
+//   rho1_a(c, c') = sum_{o in a} conj(CQ_k[c]_o)  CQ_k'[c']_o
+//   rho2_b(v', v) = sum_{o in b} conj(C_k'[v']_o) C_k[v]_o
+//   D_ij = sum_ab rho1_a V_ab rho2_b
+//     V = motif FT at the mesh point equivalent to k' - k     (real space, :893-895)
+//     V = G-summed kernel W(k - k')                           (reciprocal space, :903)
+//   X_ij = sum_a L_a(i) R_a(j)                                (exchange, :897 / :905)
+//   H_ij = -(D - X) (i < j),  H_ji = conj(H_ij),
+//   H_ii = 2 Re[(scissor + E_c - E_v)/2 - (D - X)/2]          (:909-919)
+//
+// Fast path: one thread per (k, k') pair of a 16 x 16 tile of k points; the
+// rho1 / rho2 factors are formed once per pair (not once per element as in
+// the reference) from band coefficients staged in shared memory
+// ([band][orbital][k] layout so the k' threads of a warp read consecutive
+// words).  Only tiles with kblock <= kblock' are launched; the mirror block is
+// written as the conjugate transpose, so H is exactly Hermitian.
+//
+// Precision: T = double writes the complex128 matrix (parity mode).  T = float
+// writes the mixed-precision form used by the tensor-core solver: the band
+// energies scissor + E_c - E_v as an FP64 diagonal, and the interaction
+// kernel K = H - diag in two BF16 planes, K ~= K_hi + K_lo.#pragma once
+#include "params.h"
+
+
+
+__device__ __forceinline__ void split_store(__nv_bfloat162* hi, __nv_bfloat162* lo, int64_t idx, float re, float im) {
+  const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
+  const __nv_bfloat16 lr = __float2bfloat16_rn(re - __bfloat162float(hr));
+  const __nv_bfloat16 li = __float2bfloat16_rn(im - __bfloat162float(hi_));
+  __nv_bfloat162 h; h.x = hr; h.y = hi_;
+  __nv_bfloat162 l; l.x = lr; l.y = li;
+  hi[idx] = h;
+  lo[idx] = l;
+}
+
+__device__ __forceinline__ const cd* interaction_ptr(const AsmParams& p, const AsmInputs& in, int k, int k2) {
+  int64_t e = interaction_entry(p, in.kpoints, in.kgrid, k, k2);
+  if (e < 0) {
+    atomicOr(in.status, XATU_DEVERR_INDEX);
+    e = 0;
+  }
+  return in.table + e * p.na * p.na;
+}
+
+// Writes element (i, j) (and its mirror when i != j) given D - X.
+template <typename T, bool MIXED>
+__device__ __forceinline__ void write_element(const AsmParams& p, const AsmOutputs& out, int64_t i, int64_t j,
+                                              cplx<T> dmx, double ec, double ev) {
+  if (i == j) {
+    if (MIXED) {
+      split_store(out.Khi, out.Klo, i * p.ldk + i, (float)(-dmx.x), 0.0f);
+      out.diag[i] = p.scissor + ec - ev;
+    } else {
+      const double hr = (p.scissor + ec - ev) / 2. - (double)dmx.x / 2.;
+      const double hi = -(double)dmx.y / 2.;
+      out.H[i * p.N + i] = mk(hr + hr, hi - hi);
+    }
+  } else {
+    if (MIXED) {
+      split_store(out.Khi, out.Klo, i * p.ldk + j, (float)(-dmx.x), (float)(-dmx.y));
+      split_store(out.Khi, out.Klo, j * p.ldk + i, (float)(-dmx.x), (float)(dmx.y));
+    } else {
+      out.H[i * p.N + j] = mk(-(double)dmx.x, -(double)dmx.y);
+      out.H[j * p.N + i] = mk(-(double)dmx.x, (double)dmx.y);
+    }
+  }
+}
+
+// Tiles: blockIdx.x enumerates the upper-triangular k-block pairs (kb <= kb2).
+__device__ __forceinline__ void tile_of(int t, int nblk, int& kb, int& kb2) {
+  // row kb holds nblk - kb tiles
+  int r = 0, rem = t;
+  while (rem >= nblk - r) { rem -= nblk - r; r++; }
+  kb = r;
+  kb2 = r + rem;
+}
+
+// Fast-path kernel.  CTA = a TK x TK tile of (k, k') pairs (TK = 16), one thread
+// per pair.
+//   phase 1: band coefficients of both k blocks (and the exchange factors of the
+//            tile's rows and columns) are staged in shared memory;
+//   phase 2: each thread forms T_a(v', v) = sum_b V_ab rho2_b(v', v), then for
+//            every (c, c') the conduction factors rho1_a(c, c'), and writes the
+//            final matrix values of its NC*NV x NC*NV block into a shared-memory
+//            staging tile (the V table row is read on demand through L1);
+//   phase 3: the tile and, off the diagonal, its conjugate transpose are written
+//            to HBM row by row with coalesced stores (16-byte vectors for the
+//            split-BF16 planes).
+template <typename T, int NV, int NC, int NA, bool MIXED, int TK>
+__device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out,
+                                              int nblk, int tile) {
+  constexpr int NB = NV + NC;
+  constexpr int NCV = NV * NC;
+  constexpr int TR = TK * NCV;     // rows (and columns) of the staging tile
+  constexpr int LDT = TR + 1;      // padded row pitch
+  using E = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int kb, kb2;
+  tile_of(tile, nblk, kb, kb2);
+  const int norb = p.norb;
+  const int side_sz = NB * norb * TK;
+  E* sC = reinterpret_cast<E*>(smem_raw);                  // [2][NB][norb][TK]
+  E* sTile = sC + 2 * side_sz;                             // [TR][LDT]
+  E* sL = sTile + TR * LDT;                                // [TR][NA] exchange rows
+  E* sR = sL + TR * NA;                                    // [TR][NA] exchange columns
+  const int tid = threadIdx.x;
+  const int kk = tid / TK, kk2 = tid % TK;
+  const int k = kb * TK + kk, k2 = kb2 * TK + kk2;
+  const bool active = (k < p.nk) && (k2 < p.nk) && !(kb == kb2 && k > k2);
+  // FP32 path: the pair's interaction-table row goes to registers before the
+  // staging barrier, so its L2 latency overlaps the coefficient staging.
+  constexpr bool kPrefetchV = sizeof(T) == 4;
+  E Vr[kPrefetchV ? NA : 1][kPrefetchV ? NA : 1];
+  const cd* Vt = nullptr;
+  if (active) {
+    Vt = interaction_ptr(p, in, k, k2);
+    if (kPrefetchV) {
+#pragma unroll
+      for (int a = 0; a < (kPrefetchV ? NA : 1); a++)
+#pragma unroll
+        for (int b = 0; b < (kPrefetchV ? NA : 1); b++) {
+          const cd v = Vt[a * NA + b];
+          Vr[a][b] = {(T)v.x, (T)v.y};
+        }
+    }
+  }
+#pragma unroll 4
+  for (int t = tid; t < 2 * side_sz; t += blockDim.x) {
+    const int side = t / side_sz;
+    const int r = t - side * side_sz;
+    const int band = r / (norb * TK);
+    const int r2 = r - band * norb * TK;
+    const int o = r2 / TK;
+    const int kk = r2 - o * TK;
+    const int k = (side == 0 ? kb : kb2) * TK + kk;
+    E v = {T(0), T(0)};
+    if (k < p.nk) {
+      // valence bands from the k stack, conduction bands from the k+Q stack
+      const cd c = (band < NV) ? in.eigvec[((int64_t)k * p.nb + band) * norb + o]
+                               : in.eigvecQ[((int64_t)k * p.nb + band) * norb + o];
+      v.x = (T)c.x;
+      v.y = (T)c.y;
+    }
+    sC[t] = v;
+  }
+  const int64_t row0 = (int64_t)kb * TR, col0 = (int64_t)kb2 * TR;
+  if (p.exchange) {
+    for (int t = tid; t < TR * NA; t += blockDim.x) {
+      const int r = t / NA, a = t - r * NA;
+      E l = {T(0), T(0)}, rr = {T(0), T(0)};
+      if (row0 + r < p.N) {
+        const cd x = in.exL[(row0 + r) * NA + a];
+        l.x = (T)x.x;
+        l.y = (T)x.y;
+      }
+      if (col0 + r < p.N) {
+        const cd x = in.exR[(col0 + r) * NA + a];
+        rr.x = (T)x.x;
+        rr.y = (T)x.y;
+      }
+      sL[t] = l;
+      sR[t] = rr;
+    }
+  }
+  __syncthreads();
+  if (active) {
+    const E* C1 = sC;
+    const E* C2 = sC + side_sz;
+#define SCO(S, band, o, q) (S)[((band) * norb + (o)) * TK + (q)]
+    // T_a(v', v) = sum_b V_ab rho2_b(v', v)
+    E Tm[NA][NV][NV];
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+#pragma unroll
+      for (int v2 = 0; v2 < NV; v2++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) Tm[a][v2][v] = {T(0), T(0)};
+#pragma unroll
+    for (int b = 0; b < NA; b++) {
+      E rho2[NV][NV];
+#pragma unroll
+      for (int v2 = 0; v2 < NV; v2++)
+#pragma unroll
+        for (int v = 0; v < NV; v++) rho2[v2][v] = {T(0), T(0)};
+      for (int o = p.orb_off[b]; o < p.orb_off[b + 1]; o++) {
+        E cv[NV], cv2[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+          cv[v] = SCO(C1, v, o, kk);
+          cv2[v] = SCO(C2, v, o, kk2);
+        }
+#pragma unroll
+        for (int v2 = 0; v2 < NV; v2++)
+#pragma unroll
+          for (int v = 0; v < NV; v++) cfmac(rho2[v2][v], cv2[v2], cv[v]);
+      }
+#pragma unroll
+      for (int a = 0; a < NA; a++) {
+        E V;
+        if (kPrefetchV) {
+          V = Vr[kPrefetchV ? a : 0][kPrefetchV ? b : 0];
+        } else {
+          const cd vab = Vt[a * NA + b];
+          V = {(T)vab.x, (T)vab.y};
+        }
+#pragma unroll
+        for (int v2 = 0; v2 < NV; v2++)
+#pragma unroll
+          for (int v = 0; v < NV; v++) cfma(Tm[a][v2][v], V, rho2[v2][v]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+#pragma unroll
+      for (int c2 = 0; c2 < NC; c2++) {
+        E rho1[NA];
+#pragma unroll
+        for (int a = 0; a < NA; a++) {
+          E acc = {T(0), T(0)};
+          for (int o = p.orb_off[a]; o < p.orb_off[a + 1]; o++)
+            cfmac(acc, SCO(C1, NV + c, o, kk), SCO(C2, NV + c2, o, kk2));
+          rho1[a] = acc;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+#pragma unroll
+          for (int v2 = 0; v2 < NV; v2++) {
+            const int pi = c * NV + v, pj = c2 * NV + v2;
+            if (k == k2 && pj < pi) continue;
+            E d = {T(0), T(0)};
+#pragma unroll
+            for (int a = 0; a < NA; a++) cfma(d, rho1[a], Tm[a][v2][v]);
+            const int r = kk * NCV + pi, cc = kk2 * NCV + pj;
+            if (p.exchange) {
+#pragma unroll
+              for (int a = 0; a < NA; a++) {
+                const E l = sL[r * NA + a], rr = sR[cc * NA + a];
+                d.x -= l.x * rr.x - l.y * rr.y;
+                d.y -= l.x * rr.y + l.y * rr.x;
+              }
+            }
+            E val;
+            if (k == k2 && pi == pj) {
+              const double ec = in.eigvalQ[(int64_t)k * p.nb + NV + c];
+              const double ev = in.eigval[(int64_t)k * p.nb + v];
+              if (MIXED) {
+                val.x = -d.x;
+                val.y = T(0);
+                out.diag[row0 + r] = p.scissor + ec - ev;
+              } else {
+                // H_ii = z + conj(z), z = (scissor + Ec - Ev)/2 - (D - X)/2
+                const double hr = (p.scissor + ec - ev) / 2. - (double)d.x / 2.;
+                val.x = (T)(hr + hr);
+                val.y = T(0);
+              }
+            } else {
+              val.x = -d.x;
+              val.y = -d.y;
+            }
+            sTile[r * LDT + cc] = val;
+          }
+        }
+      }
+    }
+#undef SCO
+  }
+  __syncthreads();
+  const int rows = (int)min((int64_t)TR, p.N - row0);
+  const int cols = (int)min((int64_t)TR, p.N - col0);
+  if (kb == kb2) {
+    // lower triangle of a diagonal tile = conjugate of its upper triangle
+    for (int t = tid; t < TR * TR; t += blockDim.x) {
+      const int r = t / TR, c = t - r * TR;
+      if (r > c && r < rows) {
+        const E u = sTile[c * LDT + r];
+        sTile[r * LDT + c] = E{u.x, -u.y};
+      }
+    }
+    __syncthreads();
+  }
+  if (MIXED) {
+    constexpr int VEC = 4;                  // complex elements per 16-byte store
+    constexpr int CV = (TR + VEC - 1) / VEC;
+    // direct block: rows row0 + r, columns col0 + c
+    for (int t = tid; t < TR * CV; t += blockDim.x) {
+      const int r = t / CV, c = (t - r * CV) * VEC;
+      if (r >= rows || c >= cols) continue;
+      const int64_t o = (row0 + r) * p.ldk + col0 + c;
+      if (c + VEC <= cols && (o & 3) == 0) {
+        __align__(16) __nv_bfloat162 h[VEC], l[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; q++) {
+          const E v = sTile[r * LDT + c + q];
+          const float re = (float)v.x, im = (float)v.y;
+          const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
+          h[q].x = hr;
+          h[q].y = hi_;
+          l[q].x = __float2bfloat16_rn(re - __bfloat162float(hr));
+          l[q].y = __float2bfloat16_rn(im - __bfloat162float(hi_));
+        }
+        *reinterpret_cast<uint4*>(out.Khi + o) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
+      } else {
+        for (int q = 0; q < VEC && c + q < cols; q++) {
+          const E v = sTile[r * LDT + c + q];
+          split_store(out.Khi, out.Klo, o + q, (float)v.x, (float)v.y);
+        }
+      }
+    }
+    if (kb != kb2) {
+      // mirror block: rows col0 + c, columns row0 + r, conjugate transpose
+      constexpr int RV = (TR + VEC - 1) / VEC;
+      for (int t = tid; t < TR * RV; t += blockDim.x) {
+        const int c = t / RV, r = (t - c * RV) * VEC;
+        if (c >= cols || r >= rows) continue;
+        const int64_t o = (col0 + c) * p.ldk + row0 + r;
+        if (r + VEC <= rows && (o & 3) == 0) {
+          __align__(16) __nv_bfloat162 h[VEC], l[VEC];
+#pragma unroll
+          for (int q = 0; q < VEC; q++) {
+            const E v = sTile[(r + q) * LDT + c];
+            const float re = (float)v.x, im = -(float)v.y;
+            const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
+            h[q].x = hr;
+            h[q].y = hi_;
+            l[q].x = __float2bfloat16_rn(re - __bfloat162float(hr));
+            l[q].y = __float2bfloat16_rn(im - __bfloat162float(hi_));
+          }
+          *reinterpret_cast<uint4*>(out.Khi + o) = *reinterpret_cast<const uint4*>(h);
+          *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
+        } else {
+          for (int q = 0; q < VEC && r + q < rows; q++) {
+            const E v = sTile[(r + q) * LDT + c];
+            split_store(out.Khi, out.Klo, o + q, (float)v.x, -(float)v.y);
+          }
+        }
+      }
+    }
+  } else {
+    for (int t = tid; t < TR * TR; t += blockDim.x) {
+      const int r = t / TR, c = t - r * TR;
+      if (r >= rows || c >= cols) continue;
+      const E v = sTile[r * LDT + c];
+      out.H[(row0 + r) * p.N + col0 + c] = mk((double)v.x, (double)v.y);
+    }
+    if (kb != kb2) {
+      for (int t = tid; t < TR * TR; t += blockDim.x) {
+        const int c = t / TR, r = t - c * TR;
+        if (r >= rows || c >= cols) continue;
+        const E v = sTile[r * LDT + c];
+        out.H[(col0 + c) * p.N + row0 + r] = mk((double)v.x, -(double)v.y);
+      }
+    }
+  }
+}
+

@@ -18,7 +18,12 @@ extern "C" size_t band_solve_smem(int norb, int nR, int has_overlap);
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path);
 
-// Batched persistent assembly (assembly.cu), mixed precision, one band-window class per launch.
+// Single-system tile kernels (assembly_f32.cu / assembly_f64.cu).
+cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
+                                   bool* launched);
+cudaError_t xatu_dispatch_tile_f64(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
+                                   bool* launched);
+// Batched persistent assembly (assembly_batch.cu), mixed precision, one band-window class per launch.
 bool xatu_assembly_batch_supported(int nv, int nc, int na);
 size_t xatu_assembly_batch_smem(int nv, int nc, int na, int tk, int norb, int exchange);
 cudaError_t xatu_launch_assembly_batch(int nv, int nc, int na, int tk, const AsmBatchMember* members,
