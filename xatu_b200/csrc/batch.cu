@@ -42,6 +42,7 @@
 #define BD_MAXB 16            // largest Davidson block
 #define BD_MMAX 64            // largest basis
 #define BD_EIGH_THREADS 256
+#define BD_RR_THREADS 512
 #define BD_ROT_ROWS 32
 
 struct BDav {
@@ -225,44 +226,58 @@ __global__ void __launch_bounds__(BD_ROWS) bd_cgs_update_kernel(BDGlobal g, BDav
     if (s < g.bsz) d.P[(long long)s * d.N + i] = d.P[(long long)s * d.N + i] - acc[s];
 }
 
-// V[:, 0:m] <- V[:, 0:m] Y and W likewise, BD_ROT_ROWS rows per block (staged in shared memory).
+// V[:, 0:m] <- V[:, 0:m] Y and W likewise, BD_ROT_ROWS rows per block staged in shared memory; each
+// thread accumulates a 2-row x 4-column register tile (6 shared loads per 8 complex multiply-adds).
 __global__ void __launch_bounds__(256) bd_rotate_kernel(BDGlobal g, BDav* D, const int* __restrict__ off) {
   const int mem = bd_member(off, g.nmem, blockIdx.x);
   const BDav& d = D[mem];
   if (!d.active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int LD = BD_MMAX + 1;
   const int m = d.m;
-  cd* sY = reinterpret_cast<cd*>(smem_raw);        // m x m, ld BD_MMAX
-  cd* sV = sY + BD_MMAX * BD_MMAX;                  // BD_ROT_ROWS x m (row r at r * BD_MMAX)
-  cd* sW = sV + BD_ROT_ROWS * BD_MMAX;
+  cd* sY = reinterpret_cast<cd*>(smem_raw);        // m x m, row j at j * LD
+  cd* sA = sY + BD_MMAX * LD;                       // BD_ROT_ROWS x m, row r at r * LD
   for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
     const int r = t % m, c = t / m;
-    sY[r + c * BD_MMAX] = d.Y[r + c * BD_MMAX];
+    sY[r * LD + c] = d.Y[r + c * BD_MMAX];
   }
   const long long row0 = (long long)(blockIdx.x - off[mem]) * BD_ROT_ROWS;
   const int rows = (int)min((long long)BD_ROT_ROWS, d.N - row0);
-  for (int t = threadIdx.x; t < BD_ROT_ROWS * m; t += blockDim.x) {
-    const int r = t % BD_ROT_ROWS, c = t / BD_ROT_ROWS;
-    cd v = mk(0, 0), w = mk(0, 0);
-    if (r < rows) {
-      v = d.V[(long long)c * d.N + row0 + r];
-      w = d.W[(long long)c * d.N + row0 + r];
+  const int rg = threadIdx.x >> 4, cg = threadIdx.x & 15;   // rows 2rg, 2rg+1; columns 4cg .. 4cg+3
+  for (int mat = 0; mat < 2; mat++) {
+    cd* A = mat == 0 ? d.V : d.W;
+    __syncthreads();
+    for (int t = threadIdx.x; t < BD_ROT_ROWS * m; t += blockDim.x) {
+      const int r = t % BD_ROT_ROWS, c = t / BD_ROT_ROWS;
+      sA[r * LD + c] = (r < rows) ? A[(long long)c * d.N + row0 + r] : mk(0, 0);
     }
-    sV[r * BD_MMAX + c] = v;
-    sW[r * BD_MMAX + c] = w;
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < BD_ROT_ROWS * m; t += blockDim.x) {
-    const int r = t % BD_ROT_ROWS, c = t / BD_ROT_ROWS;
-    if (r >= rows) continue;
-    cd v = mk(0, 0), w = mk(0, 0);
-    for (int j = 0; j < m; j++) {
-      const cd y = sY[j + c * BD_MMAX];
-      v = v + sV[r * BD_MMAX + j] * y;
-      w = w + sW[r * BD_MMAX + j] * y;
+    __syncthreads();
+    if (4 * cg < m) {
+      cd acc[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[i][q] = mk(0, 0);
+      for (int j = 0; j < m; j++) {
+        const cd a0 = sA[(2 * rg) * LD + j], a1 = sA[(2 * rg + 1) * LD + j];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const cd y = sY[j * LD + 4 * cg + q];
+          acc[0][q] = acc[0][q] + a0 * y;
+          acc[1][q] = acc[1][q] + a1 * y;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int r = 2 * rg + i;
+        if (r >= rows) continue;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int c = 4 * cg + q;
+          if (c < m) A[(long long)c * d.N + row0 + r] = acc[i][q];
+        }
+      }
     }
-    d.V[(long long)c * d.N + row0 + r] = v;
-    d.W[(long long)c * d.N + row0 + r] = w;
   }
 }
 
@@ -398,7 +413,7 @@ __global__ void bd_prep_kernel(BDGlobal g, BDav* D) {
 }
 
 // Hermitise the new block of T, Jacobi eigensolve, Ritz values and coefficients; m <- m + k.
-__global__ void __launch_bounds__(BD_EIGH_THREADS) bd_rr_kernel(BDGlobal g, BDav* D, int* status) {
+__global__ void __launch_bounds__(BD_RR_THREADS) bd_rr_kernel(BDGlobal g, BDav* D, int* status) {
   BDav& d = D[blockIdx.x];
   if (!d.active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -716,7 +731,7 @@ static size_t rr_smem() {
   return (size_t)m * (m + 1) * sizeof(cd) + (size_t)m * m * sizeof(cd) + (m / 2 + 2) * sizeof(JacobiRot) +
          64 * sizeof(double) + (m + 1) * sizeof(int);
 }
-static size_t rot_smem() { return (size_t)(BD_MMAX * BD_MMAX + 2 * BD_ROT_ROWS * BD_MMAX) * sizeof(cd); }
+static size_t rot_smem() { return (size_t)(BD_MMAX + BD_ROT_ROWS) * (BD_MMAX + 1) * sizeof(cd); }
 
 // One Davidson step for every active member.
 static xatu_status enqueue_iteration(xatu_batch* b) {
@@ -736,7 +751,7 @@ static xatu_status enqueue_iteration(xatu_batch* b) {
   bd_finish_append_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_prep_kernel<<<g.nmem, 256, 0, b->stream>>>(g, D);
   bd_gemm_h_kernel<<<b->nred, 256, 0, b->stream>>>(g, D, rd, 0);
-  bd_rr_kernel<<<g.nmem, BD_EIGH_THREADS, rr_smem(), b->stream>>>(g, D, status);
+  bd_rr_kernel<<<g.nmem, BD_RR_THREADS, rr_smem(), b->stream>>>(g, D, status);
   bd_rotate_kernel<<<b->nrot, 256, rot_smem(), b->stream>>>(g, D, b->d_rot_off.as<int>());
   bd_residual_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_control_kernel<<<g.nmem, 256, 0, b->stream>>>(g, D);
@@ -777,8 +792,10 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   const int nmem = (int)b->members.size();
   if (nmem == 0) return bfail(b, XATU_ERR_STATE, "empty batch");
   b->nstates = nstates;
+  // block: nstates plus guard vectors
   b->bsz = std::max(8, nstates + std::max(4, (nstates + 3) / 4));
-  if (b->bsz > BD_MAXB) return bfail(b, XATU_ERR_UNSUPPORTED, "batched Davidson supports at most 12 states");
+  if (b->bsz > BD_MAXB || b->bsz < nstates)
+    return bfail(b, XATU_ERR_UNSUPPORTED, "batched Davidson supports at most 12 states (block of 16)");
   const int mmax = std::min(BD_MMAX, 4 * b->bsz);
   // per-member buffers
   for (int i = 0; i < nmem; i++) {
