@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiation workload")
     p.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     p.add_argument("--batch-count", type=int, default=64)
+    p.add_argument("--workload", default="config2", choices=["config2", "config1", "config3"],
+                   help="config2: the headline line (default); config1 / config3: one JSON line for that workload")
     p.add_argument("--adjoint-ncell", type=int, default=48)
     return p.parse_args()
 
@@ -567,8 +569,82 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
+def config1_run() -> dict:
+    """hBN.model as shipped, Nk = 30 x 30, 1v + 1c, eps = (1, 1), r0 = 10, real-space Keldysh with the lattice
+    sum truncated at 2 |a1| (19 cells): FP64 build + dense solve on the GPU against the oracle (CPU)."""
+    import torch
+    from oracle.oracle import OracleExciton, OracleSystem
+    from xatu_b200.config import SystemConfiguration
+    from xatu_b200.exciton import ExcitonTB
+    model = os.path.join(ROOT, "tests", "golden", "models", "hBN.model")
+    cfg = SystemConfiguration(model)
+    ex = ExcitonTB(cfg, 30, 1, 0, (1.0, 1.0, 10.0))
+    ex.setCutoff(2.0)
+    ex.brillouinZoneMesh(30)
+    for rep in range(3):               # the API calls return after their device work (wall time = device time)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ex.initializeHamiltonian()
+        ex.BShamiltonian("fp64")
+        r = ex.diagonalize("diag", 8)
+        t_gpu = time.perf_counter() - t0
+    H = ex.HBS
+    si = cfg.systemInfo
+    s = OracleSystem(si.ndim, si.bravaisLattice, si.motif, si.norbitals, si.bravaisVectors, si.hamiltonian,
+                     int(si.filling))
+    o = OracleExciton(s, 30, 1, 0, (1.0, 1.0, 10.0))
+    o.cutoff = 2.0
+    o.brillouin_zone_mesh(30)
+    t0 = time.perf_counter()
+    o.initialize_hamiltonian()
+    Ho = o.bs_hamiltonian()
+    wo = np.linalg.eigvalsh(Ho)
+    t_cpu = time.perf_counter() - t0
+    ex.close()
+    return {"workload": "config1: hBN.model, Nk=30x30, 1v+1c, eps=(1,1), r0=10, real-space Keldysh, cutoff 2|a1| "
+                        f"({len(o.cells)} cells), N={o.N}",
+            "gpu_fp64_s": t_gpu, "cpu_oracle_s": t_cpu, "cpu_threads": os.cpu_count(),
+            "lowest8_eV": r.eigval[:8].tolist(), "max_abs_dE_eV_vs_oracle": float(np.abs(r.eigval[:8] - wo[:8]).max()),
+            "max_rel_H_err_vs_oracle": float(np.abs(H - Ho).max() / np.abs(Ho).max())}
+
+
+def config3_run() -> dict:
+    """The 22-orbital model in reciprocal-space mode (nG = 5 per axis, 25 G), direct + exchange, Nk = 90 x 90,
+    2v + 2c (N = 32400), lowest 16 states: the mixed path (split-BF16 K, tcgen05 Davidson, FP64
+    orthogonalisation) against the FP64 build + dense FP64 eigensolve on the same GPU."""
+    import torch
+    from xatu_b200.exciton import ExcitonTB
+    from xatu_b200.synthetic import synthetic_hexagonal
+    ex = ExcitonTB(synthetic_hexagonal(seed=1234), 90, 2, 0, (1.0, 4.5, 40.0))
+    ex.setMode("reciprocalspace")
+    ex.setReciprocalVectors(5)
+    ex.setExchange(True)
+    ex.brillouinZoneMesh(90)
+    for rep in range(3):               # the API calls return after their device work (wall time = device time)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ex.initializeHamiltonian()
+        ex.BShamiltonian("mixed")
+        rm = ex.diagonalize("davidson", 16)
+        t_mixed = time.perf_counter() - t0
+    st = ex.stageTimes()
+    t0 = time.perf_counter()
+    ex.initializeHamiltonian()
+    ex.BShamiltonian("fp64")
+    rf = ex.diagonalize("diag", 16)
+    t_fp64 = time.perf_counter() - t0
+    ex.close()
+    return {"workload": "config3: 22-orbital model, reciprocal space nG=25, direct + exchange, Nk=90x90, 2v+2c, "
+                        "N=32400, lowest 16 states",
+            "mixed_s": t_mixed, "mixed_stage_ms": st, "fp64_dense_s": t_fp64, "speedup": t_fp64 / t_mixed,
+            "max_abs_dE_eV_lowest16": float(np.abs(rm.eigval[:16] - rf.eigval[:16]).max())}
+
+
 def main():
     args = parse()
+    if args.workload != "config2":
+        print(json.dumps(config1_run() if args.workload == "config1" else config3_run()), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

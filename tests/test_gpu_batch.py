@@ -53,9 +53,10 @@ def test_batch_matches_single_system_fp64():
         assert np.abs(batch.result(i)[0] - first[i]).max() < 1e-6
     st = batch.stats()
     assert st["iterations"] > 0 and st["solve_ms"] > 0 and st["build_ms"] > 0
-    classes = {(c["nv"], c["nc"]) for c in st["tuning"]}
+    classes = {(c["nv"], c["nc"]) for c in st["tuning"]["assembly"]}
     assert classes == {(s["nv"], s["nc"]) for s in specs}
-    assert all(c["chosen_tk"] in (8, 16) for c in st["tuning"])
+    assert all(c["chosen_tk"] in (8, 16) for c in st["tuning"]["assembly"])
+    assert len(st["tuning"]["davidson"]) >= 1
     batch.close()
     for ex in exs:
         ex.close()

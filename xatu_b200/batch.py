@@ -66,7 +66,7 @@ class ExcitonBatch:
         buf = ctypes.create_string_buffer(8192)
         self._call("xatu_batch_stats", ctypes.byref(b), ctypes.byref(s), ctypes.byref(it), per, buf, 8192)
         return {"build_ms": b.value, "solve_ms": s.value, "iterations": it.value,
-                "member_iterations": list(per)[: self.size], "tuning": json.loads(buf.value.decode() or "[]")}
+                "member_iterations": list(per)[: self.size], "tuning": json.loads(buf.value.decode() or "{}")}
 
     def close(self):
         if self._b is not None:

@@ -583,6 +583,7 @@ struct xatu_batch {
   int nstates = 0, bsz = 0, max_iter = 200;
   double tol = 1e-4;
   BDGlobal g{};
+  BDGlobal chosen{};
   std::vector<BDav> hdesc;
   DBuf d_desc, d_row_off, d_red_off, d_rot_off, d_count, d_status, d_arena;
   int nrow = 0, nred = 0, nrot = 0;
@@ -771,6 +772,30 @@ static xatu_status enqueue_iteration(xatu_batch* b) {
   return XATU_OK;
 }
 
+// Build graph, then the iteration graph until no system is active; device ms of the whole solve.
+static xatu_status run_graphs(xatu_batch* b, cudaGraphExec_t build, cudaGraphExec_t iter, int* iters, float* ms) {
+  BCK(cudaEventRecord(b->ev[0], b->stream));
+  BCK(cudaGraphLaunch(build, b->stream));
+  BCK(cudaEventRecord(b->ev[1], b->stream));
+  int it = 0;
+  for (; it < b->max_iter; it++) {
+    BCK(cudaGraphLaunch(iter, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (*b->h_count == 0) {
+      it++;
+      break;
+    }
+  }
+  BCK(cudaEventRecord(b->ev[2], b->stream));
+  BCK(cudaEventSynchronize(b->ev[2]));
+  cudaEventElapsedTime(&b->build_ms, b->ev[0], b->ev[1]);
+  cudaEventElapsedTime(&b->solve_ms, b->ev[1], b->ev[2]);
+  b->iterations = it;
+  if (ms) *ms = b->build_ms + b->solve_ms;
+  if (iters) *iters = it;
+  return XATU_OK;
+}
+
 static xatu_status capture(xatu_batch* b, bool build, cudaGraphExec_t* exec) {
   cudaGraph_t graph = nullptr;
   BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
@@ -792,16 +817,23 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   const int nmem = (int)b->members.size();
   if (nmem == 0) return bfail(b, XATU_ERR_STATE, "empty batch");
   b->nstates = nstates;
-  // block: nstates plus guard vectors
-  b->bsz = std::max(8, nstates + std::max(4, (nstates + 3) / 4));
-  if (b->bsz > BD_MAXB || b->bsz < nstates)
+  // block candidates: nstates plus guard vectors, and the same rounded up to the 8-column granule of the
+  // tensor-core operand (no extra pass over K; a larger basis per iteration).  The buffers are sized for
+  // the largest; the autotuner keeps the faster.
+  const int b0 = std::max(8, nstates + std::max(4, (nstates + 3) / 4));
+  if (b0 > BD_MAXB || b0 < nstates)
     return bfail(b, XATU_ERR_UNSUPPORTED, "batched Davidson supports at most 12 states (block of 16)");
-  const int mmax = std::min(BD_MMAX, 4 * b->bsz);
+  std::vector<int> blocks = {b0};
+  if ((b0 + 7) / 8 * 8 != b0 && (b0 + 7) / 8 * 8 <= BD_MAXB) blocks.push_back((b0 + 7) / 8 * 8);
+  b->bsz = blocks.back();
+  const int mmax = BD_MMAX;
   // per-member buffers
   for (int i = 0; i < nmem; i++) {
     xatu_ctx* ctx = b->members[i];
     const long long N = ctx->N;
-    if (N < mmax) return bfail(b, XATU_ERR_UNSUPPORTED, "system " + std::to_string(i) + " is smaller than the basis");
+    if (N < std::min(BD_MMAX, 4 * b0))
+      return bfail(b, XATU_ERR_UNSUPPORTED, "system " + std::to_string(i) + " is smaller than the basis");
+    if (N < mmax) blocks.resize(1);   // the larger block's basis would not fit this system
     if (!xatu_assembly_batch_supported(ctx->nv, ctx->nc, ctx->natoms))
       return bfail(b, XATU_ERR_UNSUPPORTED, "system " + std::to_string(i) +
                                                 ": batched assembly supports 1-3 valence/conduction bands, 2-3 atoms");
@@ -839,7 +871,7 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   // Davidson arena
   b->g.nmem = nmem;
   b->g.bsz = b->bsz;
-  b->g.bp = (b->bsz + 7) / 8 * 8;
+  b->g.bp = BD_MAXB;                 // allocation: the largest operand
   b->g.mmax = mmax;
   b->g.nstates = nstates;
   b->g.max_iter = b->max_iter;
@@ -921,9 +953,41 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   BCK(xatu_raise_smem_limit((const void*)bd_rr_kernel, rr_smem()));
   BCK(xatu_raise_smem_limit((const void*)bd_rotate_kernel, rot_smem()));
   BCK(cudaStreamSynchronize(b->stream));
-  // graphs
-  BTRY(capture(b, true, &b->build_exec));
-  BTRY(capture(b, false, &b->iter_exec));
+  // graphs of every block candidate, each timed on a full solve; the fastest is kept
+  std::string dav = "";
+  float best = 1e30f;
+  for (size_t q = 0; q < blocks.size(); q++) {
+    const int bs = blocks[q];
+    b->bsz = bs;
+    b->g.bsz = bs;
+    b->g.bp = (bs + 7) / 8 * 8;
+    b->g.mmax = std::min(BD_MMAX, 4 * bs);
+    cudaGraphExec_t be = nullptr, ie = nullptr;
+    BTRY(capture(b, true, &be));
+    BTRY(capture(b, false, &ie));
+    int it = 0;
+    float ms = 0;
+    const xatu_status st = run_graphs(b, be, ie, &it, &ms);
+    char buf[160];
+    snprintf(buf, sizeof(buf), "%s{\"davidson_block\": %d, \"solve_ms\": %.3f, \"iterations\": %d}", q ? ", " : "", bs,
+             ms, it);
+    dav += buf;
+    if (st == XATU_OK && ms < best) {
+      best = ms;
+      if (b->build_exec) cudaGraphExecDestroy(b->build_exec);
+      if (b->iter_exec) cudaGraphExecDestroy(b->iter_exec);
+      b->build_exec = be;
+      b->iter_exec = ie;
+      b->chosen = b->g;
+    } else {
+      cudaGraphExecDestroy(be);
+      cudaGraphExecDestroy(ie);
+    }
+  }
+  if (!b->build_exec) return bfail(b, XATU_ERR_NOT_CONVERGED, "no Davidson block candidate converged");
+  b->g = b->chosen;
+  b->bsz = b->g.bsz;
+  b->tuning = "{\"assembly\": " + b->tuning + ", \"davidson\": [" + dav + "]}";
   b->prepared = true;
   return XATU_OK;
 }
@@ -1009,23 +1073,7 @@ xatu_status xatu_batch_run(xatu_batch* b, int nstates, double tol, int max_iter)
   } else if (nstates != b->nstates || (tol > 0 && tol != b->g.tol) || (max_iter > 0 && max_iter != b->max_iter)) {
     return bfail(b, XATU_ERR_STATE, "nstates, tol and max_iter are fixed at the first run of a batch");
   }
-  BCK(cudaEventRecord(b->ev[0], b->stream));
-  BCK(cudaGraphLaunch(b->build_exec, b->stream));
-  BCK(cudaEventRecord(b->ev[1], b->stream));
-  int it = 0;
-  for (; it < b->max_iter; it++) {
-    BCK(cudaGraphLaunch(b->iter_exec, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    if (*b->h_count == 0) {
-      it++;
-      break;
-    }
-  }
-  BCK(cudaEventRecord(b->ev[2], b->stream));
-  BCK(cudaEventSynchronize(b->ev[2]));
-  cudaEventElapsedTime(&b->build_ms, b->ev[0], b->ev[1]);
-  cudaEventElapsedTime(&b->solve_ms, b->ev[1], b->ev[2]);
-  b->iterations = it;
+  BTRY(run_graphs(b, b->build_exec, b->iter_exec, nullptr, nullptr));
   // device error words: the batch's own and every member's
   int st = 0;
   BCK(cudaMemcpy(&st, b->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
