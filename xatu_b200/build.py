@@ -61,7 +61,10 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), SOURCES))
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [_nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-lcublas", "-lcusolver"]
+        # cuBLAS / cuSOLVER of the CUDA toolkit the kernels are built with (explicit run path)
+        cudalib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(_nvcc()))), "lib64")
+        cmd = [_nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-lcublas", "-lcusolver", "-Xlinker", "-rpath",
+                                                               "-Xlinker", cudalib]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

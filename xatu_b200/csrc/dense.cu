@@ -6,6 +6,7 @@
 // H is stored row-major.  Read column-major the same buffer is H^T = conj(H)
 // (H is Hermitian), which has the same eigenvalues and conjugated
 // eigenvectors; the eigenvectors are conjugated back on the way out.
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -40,7 +41,10 @@ xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors) {
                                                      &host_ws);
   if (cs != CUSOLVER_STATUS_SUCCESS) {
     cusolverDnDestroyParams(params);
-    return xatu_fail(ctx, XATU_ERR_CUDA, "cusolverDnXsyevd_bufferSize failed");
+    return xatu_fail(ctx, vectors ? XATU_ERR_UNSUPPORTED : XATU_ERR_CUDA,
+                     std::string("cusolverDnXsyevd_bufferSize failed (status ") + std::to_string((int)cs) +
+                         ") for N = " + std::to_string(N) +
+                         (vectors ? " with eigenvectors (request eigenvalues only, or use the Davidson solver)" : ""));
   }
   cudaError_t e = ctx->dv_W.ensure(dev_ws + 16);
   if (e != cudaSuccess) {
@@ -52,7 +56,8 @@ xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors) {
                         ctx->dv_diagH.p, CUDA_C_64F, ctx->dv_W.p, dev_ws, hws.data(), host_ws,
                         ctx->dv_small.as<int>());
   cusolverDnDestroyParams(params);
-  if (cs != CUSOLVER_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cusolverDnXsyevd failed");
+  if (cs != CUSOLVER_STATUS_SUCCESS)
+    return xatu_fail(ctx, XATU_ERR_CUDA, std::string("cusolverDnXsyevd failed (status ") + std::to_string((int)cs) + ")");
   int info = 0;
   XATU_CK(cudaMemcpyAsync(&info, ctx->dv_small.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
