@@ -249,6 +249,14 @@ xatu_status xatu_stage_times(const xatu_ctx *ctx, float *ms4);
 xatu_status xatu_kernel_stats(const xatu_ctx *ctx, int which, int64_t *launches, double *total_ms, int *path);
 /* Number of engine kernels launched on this context since creation. */
 xatu_status xatu_kernel_launches(const xatu_ctx *ctx, int64_t *count);
+/* Self-test of the device eigensolver of the Davidson Rayleigh-Ritz step (no counterpart in the reference,
+   whose Davidson calls Armadillo's eig_sym on the projected matrix, davidson.cpp:30): the lowest k
+   eigenpairs of the Hermitian m x m matrix T (host, column-major complex128), m <= 112, k <= m.  Outputs
+   theta[k] ascending and Y (host, m x k column-major complex128); cycles (may be NULL): 8 SM clock stamps
+   at the solver's phase boundaries.  Allocates and frees its own device buffers; XATU_ERR_NUMERIC when the
+   solver flagged a breakdown. */
+xatu_status xatu_selftest_small_eigh(int device, int m, int k, const double *T, double *theta, double *Y,
+                                     int64_t *cycles);
 
 /* ------------------------------------------------------------------ allocation-free product */
 /* y = H x for a mixed build (FP64 diagonal + split-BF16 kernel planes), without any device allocation.

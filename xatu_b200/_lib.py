@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libxatu_bse.so")
 
 XATU_OK = 0
+XATU_ERR_INVALID = 1
 STATUS_NAMES = {0: "XATU_OK", 1: "XATU_ERR_INVALID", 2: "XATU_ERR_CUDA", 3: "XATU_ERR_NOT_CONVERGED",
                 4: "XATU_ERR_STATE", 5: "XATU_ERR_ALLOC", 6: "XATU_ERR_UNSUPPORTED", 7: "XATU_ERR_NUMERIC"}
 
@@ -33,7 +34,7 @@ EXPORTED_SYMBOLS = [
     "xatu_bse_build_basis", "xatu_adjoint", "xatu_oscillator_window_gradient", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
     "xatu_batch_set_stream", "xatu_batch_add", "xatu_batch_run", "xatu_batch_dim", "xatu_batch_result",
     "xatu_batch_stats",
-    "xatu_kernel_launches", "xatu_reciprocal_lattice", "xatu_mesh_mp", "xatu_mesh_reduced",
+    "xatu_kernel_launches", "xatu_selftest_small_eigh", "xatu_reciprocal_lattice", "xatu_mesh_mp", "xatu_mesh_reduced",
     "xatu_equivalent_points", "xatu_truncate_supercell",
 ]
 
@@ -114,6 +115,7 @@ def lib() -> ctypes.CDLL:
         "xatu_batch_result": ([vp, ci, vp, vp], ci),
         "xatu_batch_stats": ([vp, vp, vp, vp, vp, vp, ctypes.c_size_t], ci),
         "xatu_kernel_launches": ([vp, i64p], ci),
+        "xatu_selftest_small_eigh": ([ci, ci, ci, vp, vp, vp, vp], ci),
         "xatu_reciprocal_lattice": ([ci, vp, vp], ci),
         "xatu_mesh_mp": ([ci, vp, ci, vp], ci),
         "xatu_mesh_reduced": ([ci, vp, ci, ci, vp], ci),

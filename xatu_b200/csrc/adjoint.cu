@@ -50,6 +50,7 @@
 #include "kernels.h"
 
 #define ADJ_THREADS 128
+#define ADJ_WS (ADJ_THREADS + 1)   // row pitch of the per-partner weight buffer (padded against bank conflicts)
 #define ADJ_BAND_THREADS 128
 
 struct AdjParams {
@@ -99,7 +100,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
   cd* Ck = reinterpret_cast<cd*>(smem_raw);    // NB x norb (valence rows from the k stack, conduction from k + Q)
   cd* xa = Ck + NB * norb;                     // ns x NC*NV
   cd* acc = xa + ns * NC * NV;                 // ns x NB x norb
-  cd* w = acc + ns * NB * norb;                // WN x ADJ_THREADS (element-major: conflict-free stores)
+  cd* w = acc + ns * NB * norb;                // WN x ADJ_WS (element-major, padded rows)
   __shared__ double eacc[8][2];
   __shared__ int atom_of[XATU_MAX_ORB];
 
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
       double eV = 0.0, eR = 0.0;
       if (valid) {
         const cd* xs = xa + s * (NC * NV);
-        cd* wt = w + tid;   // element e of this partner at wt[e * ADJ_THREADS]
+        cd* wt = w + tid;   // element e of this partner at wt[e * ADJ_WS]
         cd xb[NC][NV];
 #pragma unroll
         for (int c2i = 0; c2i < NC; c2i++)
@@ -212,7 +213,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
                 cd t = mk(0, 0);
 #pragma unroll
                 for (int c = 0; c < NC; c++) t = t + cmulc(xs[c * NV + v], PV[c][v2]);
-                wt[(WC + (v * NA + b) * NV + v2) * ADJ_THREADS] = mk(-t.x, t.y);   // -conj(t)
+                wt[(WC + (v * NA + b) * NV + v2) * ADJ_WS] = mk(-t.x, t.y);   // -conj(t)
               }
           }
         }
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
                   t = t + cmulc(xs[c * NV + v], B[c2i][v]);
                   u = u + cmulc(xs[c * NV + v], dB[c2i][v]);
                 }
-                wt[((c * NA + a) * NC + c2i) * ADJ_THREADS] = mk(-t.x, -t.y);
+                wt[((c * NA + a) * NC + c2i) * ADJ_WS] = mk(-t.x, -t.y);
                 // Gamma-weighted sums: sum_c' P_a(c, c') (.)
                 const cd pt = P[a][c][c2i] * t, pu = P[a][c][c2i] * u;
                 eV += pt.x;
@@ -280,17 +281,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
         if (b >= NV) {
           const int c = b - NV;
           for (int q = 0; q < nq; q++) {
-            const cd* ww = w + (c * NA + a) * NC * ADJ_THREADS + q;
+            const cd* ww = w + (c * NA + a) * NC * ADJ_WS + q;
             const cd* cq = in.eigvecQ + ((int64_t)(base + q) * p.nb + NV) * norb + o;
 #pragma unroll
-            for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_THREADS] * cq[c2i * norb];
+            for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_WS] * cq[c2i * norb];
           }
         } else {
           for (int q = 0; q < nq; q++) {
-            const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_THREADS + q;
+            const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_WS + q;
             const cd* cv = in.eigvec + (int64_t)(base + q) * p.nb * norb + o;
 #pragma unroll
-            for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_THREADS] * cv[v2 * norb];
+            for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_WS] * cv[v2 * norb];
           }
         }
         acc[(s * NB + b) * norb + o] = acc[(s * NB + b) * norb + o] + sum;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_kernel(AdjParams p, AdjI
 static size_t adj_pair_smem(int nv, int nc, int na, int norb, int ns) {
   const int nb = nv + nc;
   const int wn = nc * na * nc + nv * na * nv;
-  return ((size_t)nb * norb + (size_t)ns * nc * nv + (size_t)ns * nb * norb + (size_t)ADJ_THREADS * wn) * sizeof(cd);
+  return ((size_t)nb * norb + (size_t)ns * nc * nv + (size_t)ns * nb * norb + (size_t)ADJ_WS * wn) * sizeof(cd);
 }
 
 // alpha_a = sum_i conj(x_i) L_a(i); grid (ns, na).
@@ -766,7 +767,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_weight_kernel(AdjParams 
   const int norb = p.norb, k = blockIdx.x, tid = threadIdx.x;
   cd* Ck = reinterpret_cast<cd*>(smem_raw);    // NB x norb
   cd* acc = Ck + NB * norb;                    // NB x norb
-  cd* w = acc + NB * norb;                     // (WC + NV NA NV) x ADJ_THREADS
+  cd* w = acc + NB * norb;                     // (WC + NV NA NV) x ADJ_WS
   __shared__ int atom_of[XATU_MAX_ORB];
   for (int t = tid; t < NB * norb; t += ADJ_THREADS) {
     const int b = t / norb;
@@ -850,7 +851,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_weight_kernel(AdjParams 
             for (int v = 0; v < NV; v++)
 #pragma unroll
               for (int v2 = 0; v2 < NV; v2++) t = t + Yb[c * NV + v][c2i * NV + v2] * VR[v2][v];
-            wt[((c * NA + a) * NC + c2i) * ADJ_THREADS] = mk(-t.x, -t.y);
+            wt[((c * NA + a) * NC + c2i) * ADJ_WS] = mk(-t.x, -t.y);
           }
       }
       // wv[v][b][v'] = -sum_{c,c'} conj(Y[cv][c'v']) conj(sum_a P_a(c, c') V_ab)
@@ -875,7 +876,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_weight_kernel(AdjParams 
             for (int c = 0; c < NC; c++)
 #pragma unroll
               for (int c2i = 0; c2i < NC; c2i++) t = t + Yb[c * NV + v][c2i * NV + v2] * PV[c][c2i];
-            wt[(WC + (v * NA + b) * NV + v2) * ADJ_THREADS] = mk(-t.x, t.y);   // -conj(t)
+            wt[(WC + (v * NA + b) * NV + v2) * ADJ_WS] = mk(-t.x, t.y);   // -conj(t)
           }
       }
     }
@@ -886,17 +887,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_pair_weight_kernel(AdjParams 
       if (b >= NV) {
         const int c = b - NV;
         for (int q = 0; q < nq; q++) {
-          const cd* ww = w + (c * NA + a) * NC * ADJ_THREADS + q;
+          const cd* ww = w + (c * NA + a) * NC * ADJ_WS + q;
           const cd* cq = in.eigvecQ + ((int64_t)(base + q) * p.nb + NV) * norb + o;
 #pragma unroll
-          for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_THREADS] * cq[c2i * norb];
+          for (int c2i = 0; c2i < NC; c2i++) sum = sum + ww[c2i * ADJ_WS] * cq[c2i * norb];
         }
       } else {
         for (int q = 0; q < nq; q++) {
-          const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_THREADS + q;
+          const cd* ww = w + (WC + (b * NA + a) * NV) * ADJ_WS + q;
           const cd* cv = in.eigvec + (int64_t)(base + q) * p.nb * norb + o;
 #pragma unroll
-          for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_THREADS] * cv[v2 * norb];
+          for (int v2 = 0; v2 < NV; v2++) sum = sum + ww[v2 * ADJ_WS] * cv[v2 * norb];
         }
       }
       acc[t] = acc[t] + sum;
@@ -949,7 +950,7 @@ static cudaError_t launch_weight(const AdjParams& p, const AdjInputs& in, const 
                                  double* ebar, cudaStream_t st) {
   const int nb = NV + NC;
   const int wn = NC * NA * NC + NV * NA * NV;
-  const size_t smem = ((size_t)2 * nb * p.norb + (size_t)ADJ_THREADS * wn) * sizeof(cd);
+  const size_t smem = ((size_t)2 * nb * p.norb + (size_t)ADJ_WS * wn) * sizeof(cd);
   cudaError_t e = xatu_raise_smem_limit((const void*)adj_pair_weight_kernel<NV, NC, NA>, smem);
   if (e != cudaSuccess) return e;
   adj_pair_weight_kernel<NV, NC, NA><<<p.nk, ADJ_THREADS, smem, st>>>(p, in, wi, cbar, ebar);

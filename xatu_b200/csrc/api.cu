@@ -815,6 +815,7 @@ xatu_status xatu_kernel_matvec(xatu_ctx* ctx, int nvec, const double* X, double*
   if (st != XATU_OK) return st;
   XATU_CK(cudaMemcpyAsync(Y, ctx->dv_W.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
+  xatu_hx_collect(ctx);
   int dst = 0;
   XATU_CK(cudaMemcpy(&dst, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (dst) {

@@ -8,7 +8,9 @@
 //     (the reference starts from the first identity columns, davidson.cpp:19);
 //   * H.V: mixed build -> diag(E) V in FP64 plus K V with K = K_hi + K_lo
 //     (split BF16, FP32 accumulation); FP64 build -> ZGEMM on the FP64 matrix;
-//   * Rayleigh-Ritz in FP64: T = V^H (H V), Jacobi eigensolve on the device;
+//   * Rayleigh-Ritz in FP64: T = V^H (H V) grown by the new columns only, the
+//     lowest block of its eigenpairs by a one-CTA Householder / multisection /
+//     inverse-iteration solver (eigh_small.cuh);
 //   * residuals r = H u - theta u in FP64, per-row diagonal preconditioner
 //     t = r / (theta - H_ii) (the reference divides by H_jj of the state
 //     index j, davidson.cpp:36-40);
@@ -23,9 +25,8 @@
 #include <vector>
 
 #include "engine.h"
-#include "jacobi.cuh"
+#include "eigh_small.cuh"
 
-#define DAV_EIGH_THREADS 512
 #define DAV_MAX_BASIS 112
 
 // ---------------------------------------------------------------- kernels
@@ -102,30 +103,12 @@ __global__ void dav_set_diag_kernel(cd* T, int ld, int k, const double* theta) {
   T[r + (long long)c * ld] = mk(r == c ? theta[r] : 0.0, 0.0);
 }
 
-// One-block eigensolve of T (m x m, column-major ld) -> theta ascending, Y column-major ld (sorted).
-__global__ void __launch_bounds__(DAV_EIGH_THREADS)
-dav_small_eigh_kernel(const cd* __restrict__ T, int ld, int m, double* __restrict__ theta, cd* __restrict__ Y,
-                      cd* __restrict__ Vscratch, int max_sweeps, int* __restrict__ status) {
+// Rayleigh-Ritz eigensolve: lowest k eigenpairs of T (m x m, column-major ldt), one CTA (eigh_small.cuh).
+__global__ void __launch_bounds__(HEEV_THREADS)
+dav_heev_kernel(const cd* __restrict__ T, int ldt, int m, int k, double* __restrict__ theta, cd* __restrict__ Y,
+                int ldy, cd* __restrict__ refl, int* __restrict__ status, long long* __restrict__ prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lda = m + 1;
-  cd* A = reinterpret_cast<cd*>(smem_raw);
-  JacobiRot* rot = reinterpret_cast<JacobiRot*>(A + (size_t)m * lda);
-  double* scratch = reinterpret_cast<double*>(rot + (m / 2 + 2));
-  int* perm = reinterpret_cast<int*>(scratch + 64);
-  BlockGroup g;
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int r = t / m, c = t - r * m;
-    A[r * lda + c] = T[r + (long long)c * ld];
-  }
-  __syncthreads();
-  const int sweeps = jacobi_eigh(g, A, lda, Vscratch, m, m, rot, scratch, max_sweeps, 1e-14);
-  if (sweeps > max_sweeps && threadIdx.x == 0) atomicOr(status, XATU_DEVERR_NOCONV);
-  jacobi_sort(g, A, lda, m, perm);
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int c = t / m, r = t - c * m;   // column c of the sorted output
-    Y[r + (long long)c * ld] = Vscratch[r * m + perm[c]];
-  }
-  for (int c = threadIdx.x; c < m; c += blockDim.x) theta[c] = A[perm[c] * lda + perm[c]].x;
+  heev_lowest(T, ldt, m, k, theta, Y, ldy, refl, smem_raw, status, prof);
 }
 
 // R[:, s] = WU[:, s] - theta[s] U[:, s]; norms[s] = ||R[:, s]||  (one block per column)
@@ -295,18 +278,13 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
           V, N, col0 + c, b, bp, ldb, ctx->dv_Bop.as<__nv_bfloat16>(), ctx->dv_Blo.as<__nv_bfloat16>());
       ctx->launches++;
       XATU_CK(cudaGetLastError());
-      XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+      if (c == 0) XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
       XATU_CK(xatu_launch_hx_tc(ctx->d_Khi.p, ctx->d_Klo.p, N, ctx->ldk, ctx->dv_Bop.p, ctx->dv_Blo.p, ldb, ng,
                                 ctx->dv_Yf.as<float>(), ctx->d_status.as<int>(), ctx->num_sms, ctx->stream));
-      XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
-      XATU_CK(cudaEventSynchronize(ctx->ev[9]));
-      {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]);
-        ctx->hx_ms += ms;
-        ctx->hx_calls++;
-        ctx->hx_last_path = 2;
-      }
+      if (c + 32 >= nv) XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+      ctx->hx_pending = true;
+      ctx->hx_calls++;
+      ctx->hx_last_path = 2;
       ctx->launches++;
       const long long tw = N * b;
       dav_finish_w_tc_kernel<<<(int)((tw + threads - 1) / threads), threads, 0, ctx->stream>>>(
@@ -324,18 +302,13 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
     const int blocks = (int)((tot + threads - 1) / threads);
     dav_gather_f32_kernel<<<blocks, threads, 0, ctx->stream>>>(V, N, col0 + c, b, ctx->dv_X.as<float2>());
     ctx->launches++;
-    XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
+    if (c == 0) XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
     XATU_CK(xatu_launch_hx_cuda_core(ctx->d_Khi.as<__nv_bfloat162>(), ctx->d_Klo.as<__nv_bfloat162>(), ctx->ldk,
                                      ctx->dv_X.as<float2>(), ctx->dv_Yf.as<float2>(), N, b, ctx->stream));
-    XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
-    XATU_CK(cudaEventSynchronize(ctx->ev[9]));
-    {
-      float ms = 0;
-      cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]);
-      ctx->hx_ms += ms;
-      ctx->hx_calls++;
-      ctx->hx_last_path = 1;
-    }
+    if (c + 32 >= nv) XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+    ctx->hx_pending = true;
+    ctx->hx_calls++;
+    ctx->hx_last_path = 1;
     ctx->launches++;
     dav_finish_w_kernel<<<blocks, threads, 0, ctx->stream>>>(ctx->dv_Yf.as<float2>(), ctx->d_diag.as<double>(), V, N,
                                                              col0 + c, b, W);
@@ -343,6 +316,13 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
     XATU_CK(cudaGetLastError());
   }
   return XATU_OK;
+}
+
+void xatu_hx_collect(xatu_ctx* ctx) {
+  if (!ctx->hx_pending) return;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, ctx->ev[8], ctx->ev[9]) == cudaSuccess) ctx->hx_ms += ms;
+  ctx->hx_pending = false;
 }
 
 static xatu_status zgemm(xatu_ctx* ctx, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
@@ -411,7 +391,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   const bool mixed = ctx->built_prec == XATU_PREC_MIXED;
   // block = nstates plus guard vectors (at least 4), so that a state of a dense spectrum cannot drop out
   // of the block unnoticed while every residual of the block looks converged; only the first nstates must
-  // converge.  The Rayleigh-Ritz cost grows with the cube of the basis (at most 4 blocks).
+  // converge.  The basis holds at most 4 blocks.
   int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(4, (nstates + 3) / 4));
   bsz = std::max(bsz, nstates);
   bsz = (int)std::min<long long>(bsz, N);
@@ -424,21 +404,24 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   XATU_CK(ctx->dv_V.ensure(vbytes));
   XATU_CK(ctx->dv_W.ensure(vbytes));
   XATU_CK(ctx->dv_R.ensure((size_t)N * bsz * sizeof(cd)));
+  XATU_CK(ctx->dv_U.ensure((size_t)2 * N * bsz * sizeof(cd)));
   XATU_CK(ctx->dv_tmp.ensure((size_t)N * mmax * sizeof(cd)));
-  XATU_CK(ctx->dv_T.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd) * 2 + 4096));
+  XATU_CK(ctx->dv_T.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd) * 3 + 4096));
   XATU_CK(ctx->dv_G.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd)));
   XATU_CK(ctx->dv_diagH.ensure((size_t)N * sizeof(double)));
   XATU_CK(ctx->dv_norm.ensure(4096 * sizeof(double)));
   cd* V = ctx->dv_V.as<cd>();
   cd* W = ctx->dv_W.as<cd>();
   cd* R = ctx->dv_R.as<cd>();
+  cd* U = ctx->dv_U.as<cd>();                           // Ritz vectors V Y (N x bsz)
+  cd* WU = U + (size_t)N * bsz;                         // W Y
   const int ldT = DAV_MAX_BASIS;
-  cd* T = ctx->dv_T.as<cd>();
-  cd* Yr = T + (size_t)ldT * ldT;                       // Ritz coefficient matrix (ldT x ldT)
+  cd* T = ctx->dv_T.as<cd>();                           // projected matrix V^H H V (ldT x ldT)
+  cd* Yr = T + (size_t)ldT * ldT;                       // Ritz coefficients (ldT x bsz)
+  cd* refl = Yr + (size_t)ldT * ldT;                    // reflectors of the small eigensolver
   double* theta = ctx->dv_norm.as<double>();            // [0, 256)
   double* norms = theta + 256;                          // [256, 512)
   int* sel_dev = reinterpret_cast<int*>(theta + 512);   // ints
-  cd* Vscratch = ctx->dv_G.as<cd>();                    // Jacobi eigenvectors (row-major m x m)
   double* diagH = ctx->dv_diagH.as<double>();
   const int threads = 256;
   // diagonal of H
@@ -467,17 +450,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     ctx->launches++;
     XATU_CK(cudaGetLastError());
   }
-  // the small eigensolver's shared memory
-  const size_t eigh_smem_max = (size_t)DAV_MAX_BASIS * (DAV_MAX_BASIS + 1) * sizeof(cd) +
-                               (DAV_MAX_BASIS / 2 + 2) * sizeof(JacobiRot) + 64 * sizeof(double) +
-                               (DAV_MAX_BASIS + 1) * sizeof(int);
-  XATU_CK(xatu_raise_smem_limit((const void*)dav_small_eigh_kernel, eigh_smem_max));
+  XATU_CK(xatu_raise_smem_limit((const void*)dav_heev_kernel, heev_smem_bytes(DAV_MAX_BASIS, DAV_MAX_BASIS / 2)));
 
-  // The basis V (and W = H V) is kept in Ritz form: after every Rayleigh-Ritz
-  // step V <- V Y, W <- W Y and T <- diag(theta), so the projected matrix of
-  // the next step is diagonal except for the rows and columns of the new
-  // corrections, and its Jacobi solve converges in a few sweeps.  A restart is
-  // a truncation to the lowest `bsz` Ritz vectors.
+  // Thick-restart block Davidson on the basis V (W = H V):
+  //   T[:, new] = V^H W[:, new] (the old block of T is kept);  lowest nritz Ritz pairs of T;
+  //   U = V Y, WU = W Y, residuals WU - U theta;  corrections appended after orthonormalisation;
+  //   restart: V <- U, W <- WU, T <- diag(theta).
   int m0 = 0, m = bsz;
   int it = 0;
   bool converged = false;
@@ -488,12 +466,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   ctx->dav_maxres = 0;
   ctx->hx_calls = 0;
   ctx->hx_ms = 0;
-  cd* tmp = ctx->dv_tmp.as<cd>();
+  ctx->hx_pending = false;
   for (it = 0; it < ctx->dav_max_iter; it++) {
     const int nnew = m - m0;
     // 1. W for the new columns
     XATU_TRY(xatu_apply_h(ctx, N, m0, nnew));
-    // 2. new columns of T = V^H W; the old block is already diag(theta)
+    // 2. new columns of T = V^H W
     XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nnew, (int)N, &kOne, V, (int)N, W + (long long)m0 * N, (int)N,
                    &kZero, T + (long long)m0 * ldT, ldT));
     {
@@ -502,33 +480,24 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK(cudaGetLastError());
     }
-    // 3. Rayleigh-Ritz
-    {
-      const size_t smem = (size_t)m * (m + 1) * sizeof(cd) + (m / 2 + 2) * sizeof(JacobiRot) + 64 * sizeof(double) +
-                          (m + 1) * sizeof(int);
-      dav_small_eigh_kernel<<<1, DAV_EIGH_THREADS, smem, ctx->stream>>>(T, ldT, m, theta, Yr, Vscratch, 60,
-                                                                         ctx->d_status.as<int>());
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-    }
-    // 4. rotate the basis into Ritz form (FP64 ZGEMMs through scratch)
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, m, m, &kOne, V, (int)N, Yr, ldT, &kZero, tmp, (int)N));
-    XATU_CK(cudaMemcpyAsync(V, tmp, sizeof(cd) * (size_t)N * m, cudaMemcpyDeviceToDevice, ctx->stream));
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, m, m, &kOne, W, (int)N, Yr, ldT, &kZero, tmp, (int)N));
-    XATU_CK(cudaMemcpyAsync(W, tmp, sizeof(cd) * (size_t)N * m, cudaMemcpyDeviceToDevice, ctx->stream));
-    dav_set_diag_kernel<<<(m * m + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, theta);
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
+    // 3. Rayleigh-Ritz: the lowest nritz eigenpairs of T
     const int nritz = std::min(bsz, m);
-    // 5. residuals of the lowest Ritz pairs
-    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(V, W, theta, N, R, norms);
+    dav_heev_kernel<<<1, HEEV_THREADS, heev_smem_bytes(m, nritz), ctx->stream>>>(T, ldT, m, nritz, theta, Yr, ldT,
+                                                                                  refl, ctx->d_status.as<int>(), nullptr);
     ctx->launches++;
     XATU_CK(cudaGetLastError());
-    XATU_CK(cudaMemcpyAsync(h_theta.data(), theta, m * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // 4. Ritz vectors and residuals
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, V, (int)N, Yr, ldT, &kZero, U, (int)N));
+    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, W, (int)N, Yr, ldT, &kZero, WU, (int)N));
+    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(U, WU, theta, N, R, norms);
+    ctx->launches++;
+    XATU_CK(cudaGetLastError());
+    XATU_CK(cudaMemcpyAsync(h_theta.data(), theta, nritz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     XATU_CK(cudaMemcpyAsync(h_norm.data(), norms, nritz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     int st = 0;
     XATU_CK(cudaMemcpyAsync(&st, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     XATU_CK(cudaStreamSynchronize(ctx->stream));
+    xatu_hx_collect(ctx);
     if (st) {
       cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream);
       return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz or K.X stage reported an error");
@@ -546,13 +515,18 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     }
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     if (el > wall_cap_s) break;
-    // 6. correction targets: unconverged among the lowest Ritz pairs
+    // 5. correction targets: unconverged among the lowest Ritz pairs
     std::vector<int> sel;
     for (int s = 0; s < nritz; s++)
       if (h_norm[s] >= tol) sel.push_back(s);
     int nsel = (int)sel.size();
-    // 7. restart = truncation (the basis is already in Ritz order)
+    // 6. thick restart on the Ritz vectors
     if (m + nsel > mmax) {
+      XATU_CK(cudaMemcpyAsync(V, U, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
+      XATU_CK(cudaMemcpyAsync(W, WU, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
+      dav_set_diag_kernel<<<(nritz * nritz + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, nritz, theta);
+      ctx->launches++;
+      XATU_CK(cudaGetLastError());
       m = nritz;
       if (m + nsel > mmax) nsel = mmax - m;
     }
@@ -571,10 +545,10 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     m0 = m;
     m += kept;
   }
-  // results: the basis is in Ritz order, its first columns are the eigenvectors
+  // results: the Ritz vectors of the last Rayleigh-Ritz step
   std::copy(h_theta.begin(), h_theta.begin() + nstates, eigval);
   if (eigvec)
-    XATU_CK(cudaMemcpyAsync(eigvec, V, sizeof(cd) * (size_t)N * nstates, cudaMemcpyDeviceToHost, ctx->stream));
+    XATU_CK(cudaMemcpyAsync(eigvec, U, sizeof(cd) * (size_t)N * nstates, cudaMemcpyDeviceToHost, ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   if (!converged) {
     char buf[160];
@@ -583,4 +557,46 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, buf);
   }
   return XATU_OK;
+}
+
+// Lowest k eigenpairs of a Hermitian matrix given on the host (column-major, m x m) through the device
+// solver of the Rayleigh-Ritz step.  Self-test of that solver; allocates and frees its own buffers.
+extern "C" xatu_status xatu_selftest_small_eigh(int device, int m, int k, const double* T, double* theta,
+                                                double* Y, int64_t* cycles) {
+  if (m < 1 || m > HEEV_MAXM || k < 1 || k > m || !T || !theta || !Y) return XATU_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return XATU_ERR_CUDA;
+  cd *dT = nullptr, *dY = nullptr, *dR = nullptr;
+  double* dth = nullptr;
+  int* dst = nullptr;
+  long long* dprof = nullptr;
+  xatu_status out = XATU_OK;
+  const size_t mm = (size_t)m * m * sizeof(cd);
+  int hst = 0;
+  if (cudaMalloc(&dT, mm) != cudaSuccess || cudaMalloc(&dY, mm) != cudaSuccess || cudaMalloc(&dR, mm) != cudaSuccess ||
+      cudaMalloc(&dth, (size_t)m * sizeof(double)) != cudaSuccess || cudaMalloc(&dst, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&dprof, 8 * sizeof(long long)) != cudaSuccess) {
+    out = XATU_ERR_CUDA;
+  } else {
+    const size_t smem = heev_smem_bytes(m, k);
+    bool ok = cudaMemcpy(dT, T, mm, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemset(dst, 0, sizeof(int)) == cudaSuccess &&
+              xatu_raise_smem_limit((const void*)dav_heev_kernel, smem) == cudaSuccess;
+    if (ok) {
+      dav_heev_kernel<<<1, HEEV_THREADS, smem>>>(dT, m, m, k, dth, dY, m, dR, dst, cycles ? dprof : nullptr);
+      ok = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+           cudaMemcpy(theta, dth, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
+           cudaMemcpy(Y, dY, (size_t)m * k * sizeof(cd), cudaMemcpyDeviceToHost) == cudaSuccess &&
+           cudaMemcpy(&hst, dst, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess &&
+           (!cycles || cudaMemcpy(cycles, dprof, 8 * sizeof(long long), cudaMemcpyDeviceToHost) == cudaSuccess);
+    }
+    if (!ok) out = XATU_ERR_CUDA;
+    else if (hst) out = XATU_ERR_NUMERIC;
+  }
+  cudaFree(dT);
+  cudaFree(dY);
+  cudaFree(dR);
+  cudaFree(dth);
+  cudaFree(dst);
+  cudaFree(dprof);
+  return out;
 }

@@ -90,6 +90,7 @@ struct xatu_ctx {
   long long hx_calls = 0;     // K.X launches of the last solve
   double hx_ms = 0;           // their summed device time
   int hx_last_path = -1;      // 1 CUDA cores, 2 tcgen05
+  bool hx_pending = false;    // ev[8]..ev[9] bracket K.X launches not yet added to hx_ms
   int num_sms = 148;
   int dav_iters = 0;
   double dav_maxres = 0;
@@ -161,6 +162,8 @@ cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, lon
 size_t xatu_hx_tc_smem(int ng);
 // W[:, col0 : col0 + nv] = H V[:, col0 : col0 + nv] with the current build (davidson.cu).
 xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv);
+// Adds the bracketed K.X device time of the last xatu_apply_h to hx_ms (call after a stream synchronisation).
+void xatu_hx_collect(xatu_ctx* ctx);
 
 // After a kernel launch: the launch's own error, labelled with the kernel.
 #define XATU_CK_LAUNCH(name)                                                       \
