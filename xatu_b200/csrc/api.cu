@@ -106,8 +106,10 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->dv_X, &ctx->dv_Yf, &ctx->dv_G, &ctx->dv_tmp, &ctx->dv_diagH, &ctx->dv_small,
                   &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo, &ctx->d_adjX, &ctx->d_adjdvtab,
                   &ctx->d_adjdtable, &ctx->d_adjdVX, &ctx->d_adjAlpha, &ctx->d_adjExUW, &ctx->d_adjCbar,
-                  &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG, &ctx->d_oscG};
+                  &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG, &ctx->d_oscG,
+                  &ctx->dv_part};
   for (DBuf* b : bufs) b->release();
+  if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
   for (auto& e : ctx->ev)

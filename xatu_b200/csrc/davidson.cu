@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "dav_tall.cuh"
 #include "eigh_small.cuh"
 
 #define DAV_MAX_BASIS 112
@@ -109,102 +110,6 @@ dav_heev_kernel(const cd* __restrict__ T, int ldt, int m, int k, double* __restr
                 int ldy, cd* __restrict__ refl, int* __restrict__ status, long long* __restrict__ prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   heev_lowest(T, ldt, m, k, theta, Y, ldy, refl, smem_raw, status, prof);
-}
-
-// R[:, s] = WU[:, s] - theta[s] U[:, s]; norms[s] = ||R[:, s]||  (one block per column)
-__global__ void dav_residual_kernel(const cd* __restrict__ U, const cd* __restrict__ WU, const double* __restrict__ theta,
-                                    long long N, cd* __restrict__ R, double* __restrict__ norms) {
-  const int s = blockIdx.x;
-  const double th = theta[s];
-  double acc = 0.0;
-  for (long long i = threadIdx.x; i < N; i += blockDim.x) {
-    const long long o = (long long)s * N + i;
-    const cd u = U[o], w = WU[o];
-    const cd r = mk(w.x - th * u.x, w.y - th * u.y);
-    R[o] = r;
-    acc += nrm2(r);
-  }
-  __shared__ double red[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s2 = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s2 += red[w];
-    norms[s] = sqrt(s2);
-  }
-}
-
-// V[:, col0 + j] = R[:, sel[j]] / (theta[sel[j]] - diagH)
-__global__ void dav_precondition_kernel(const cd* __restrict__ R, const double* __restrict__ theta,
-                                        const double* __restrict__ diagH, const int* __restrict__ sel, int nsel,
-                                        long long N, cd* __restrict__ V, int col0) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= N * nsel) return;
-  const int j = (int)(t / N);
-  const long long i = t - (long long)j * N;
-  const int s = sel[j];
-  double den = theta[s] - diagH[i];
-  if (fabs(den) < 1e-8) den = (den < 0 ? -1e-8 : 1e-8);
-  const cd r = R[(long long)s * N + i];
-  V[(long long)(col0 + j) * N + i] = mk(r.x / den, r.y / den);
-}
-
-// ---------------------------------------------------------------- host helpers
-struct Z {
-  double x, y;
-};
-
-static const cuDoubleComplex kOne = {1.0, 0.0}, kZero = {0.0, 0.0}, kMinusOne = {-1.0, 0.0};
-
-// Pivoted Cholesky of the Hermitian Gram matrix G (n x n, column-major) ->
-// S (n x k, column-major) with S^H G S = I over the kept directions.  Columns
-// whose remaining norm falls below rel * max diag are dropped.
-static int gram_to_orthonormalizer(const std::vector<Z>& G, int n, double rel, std::vector<Z>& S) {
-  // Modified Gram-Schmidt in the G inner product, column by column.
-  std::vector<Z> B(n * n, Z{0, 0});  // columns of B are coefficient vectors
-  std::vector<int> kept;
-  double maxd = 0;
-  for (int i = 0; i < n; i++) maxd = std::max(maxd, G[i + i * n].x);
-  auto gdot = [&](const Z* a, const Z* b) {  // a^H G b
-    Z s{0, 0};
-    for (int r = 0; r < n; r++) {
-      Z gb{0, 0};
-      for (int c = 0; c < n; c++) {
-        const Z g = G[r + c * n];
-        gb.x += g.x * b[c].x - g.y * b[c].y;
-        gb.y += g.x * b[c].y + g.y * b[c].x;
-      }
-      s.x += a[r].x * gb.x + a[r].y * gb.y;
-      s.y += a[r].x * gb.y - a[r].y * gb.x;
-    }
-    return s;
-  };
-  std::vector<Z> cols;
-  for (int j = 0; j < n; j++) {
-    std::vector<Z> v(n, Z{0, 0});
-    v[j] = Z{1, 0};
-    for (int pass = 0; pass < 2; pass++)
-      for (size_t q = 0; q < cols.size() / n; q++) {
-        const Z* u = &cols[q * n];
-        const Z c = gdot(u, v.data());
-        for (int r = 0; r < n; r++) {
-          v[r].x -= c.x * u[r].x - c.y * u[r].y;
-          v[r].y -= c.x * u[r].y + c.y * u[r].x;
-        }
-      }
-    const double nn = gdot(v.data(), v.data()).x;
-    if (nn <= rel * maxd || nn <= 0) continue;
-    const double f = 1.0 / std::sqrt(nn);
-    for (int r = 0; r < n; r++) {
-      v[r].x *= f;
-      v[r].y *= f;
-    }
-    cols.insert(cols.end(), v.begin(), v.end());
-  }
-  S = cols;
-  return (int)(cols.size() / n);
 }
 
 // Bt operand of the tensor-core product (hx_tc.cu) from V[:, col0 : col0 + b]:
@@ -325,59 +230,87 @@ void xatu_hx_collect(xatu_ctx* ctx) {
   ctx->hx_pending = false;
 }
 
-static xatu_status zgemm(xatu_ctx* ctx, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
-                         const cuDoubleComplex* alpha, const cd* A, int lda, const cd* B, int ldb,
-                         const cuDoubleComplex* beta, cd* C, int ldc) {
-  cublasStatus_t s = cublasZgemm(ctx->blas, ta, tb, m, n, k, alpha, reinterpret_cast<const cuDoubleComplex*>(A), lda,
-                                 reinterpret_cast<const cuDoubleComplex*>(B), ldb, beta,
-                                 reinterpret_cast<cuDoubleComplex*>(C), ldc);
-  if (s != CUBLAS_STATUS_SUCCESS) return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZgemm failed");
-  return XATU_OK;
-}
-
 #define XATU_TRY(x)                  \
   do {                               \
     xatu_status s__ = (x);           \
     if (s__ != XATU_OK) return s__;  \
   } while (0)
 
-// Orthonormalise V[:, m : m + nsel] against V[:, 0 : m] and within itself.
-// Returns the number of vectors kept (moved to V[:, m : m + kept]).
+// Row-tile height for a kernel whose shared memory is smem(TR): 64 rows while that fits in 100 KB, else the
+// largest of 32 / 16 (min_tr at least) within 200 KB.
+template <typename F>
+static int ts_pick_tile(F smem, int min_tr) {
+  if (smem(64) <= 100 * 1024) return 64;
+  if (smem(32) <= 200 * 1024 || min_tr >= 32) return 32;
+  return 16;
+}
+
+static xatu_status ts_part_ensure(xatu_ctx* ctx, size_t bytes) {
+  if (ctx->dv_part.bytes < bytes) XATU_CK(ctx->dv_part.ensure(bytes));
+  return XATU_OK;
+}
+
+// Z[0:a, 0:b] (leading dimension ldz) = A[:, 0:a]^H B[:, 0:b] over N rows: per-tile partials, then their
+// ordered sum.  status_out (may be NULL) gets a copy of the device status word.
+static xatu_status ts_proj(xatu_ctx* ctx, const cd* A, int a, const cd* B, int b, long long N, cd* Z, int ldz,
+                           double* status_out = nullptr) {
+  if (a <= 0 || b <= 0) return XATU_OK;
+  const int TR = ts_pick_tile([&](int tr) { return ts_proj_smem(a, b, tr); }, 16);
+  const int G = (int)((N + TR - 1) / TR);
+  const int ab = a * b;
+  XATU_TRY(ts_part_ensure(ctx, (size_t)G * ab * sizeof(cd)));
+  ts_proj_kernel<<<G, TS_THREADS, ts_proj_smem(a, b, TR), ctx->stream>>>(A, a, B, b, N, TR, ctx->dv_part.as<cd>());
+  ctx->launches++;
+  XATU_CK_LAUNCH("ts_proj_kernel");
+  ts_sum_kernel<<<(ab + 31) / 32, TS_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, ab, a, Z, ldz,
+                                                                 ctx->d_status.as<int>(), status_out);
+  ctx->launches++;
+  XATU_CK_LAUNCH("ts_sum_kernel");
+  return XATU_OK;
+}
+
+// Out[:, 0:b] = (In[:, 0:b] - A[:, 0:a] C) S over N rows (A NULL: no projection; S NULL: identity).
+static xatu_status ts_update(xatu_ctx* ctx, const cd* In, int b, const cd* A, int a, const cd* C, int ldc,
+                             const cd* S, cd* Out, long long N) {
+  const int TR = ts_pick_tile([&](int tr) { return ts_update_smem(a, b, tr); }, 16);
+  const int G = (int)((N + TR - 1) / TR);
+  ts_update_kernel<<<G, TS_THREADS, ts_update_smem(a, b, TR), ctx->stream>>>(In, b, A, a, C, ldc, S, Out, N, TR);
+  ctx->launches++;
+  XATU_CK_LAUNCH("ts_update_kernel");
+  return XATU_OK;
+}
+
+// Orthonormalise the block t = V[:, m : m + nsel] against V[:, 0 : m] and within itself:
+//   t <- t - V (V^H t);
+//   Z = [V t]^H t: C = V^H t, G = t^H t - C^H C; Cholesky of G with dropping -> S;  X = (t - V C) S;
+//   G = X^H X -> S (second Cholesky pass, absolute threshold);  t <- X S.
+// The kept directions end in V[:, m : m + kept], the rest of the block is zero; `kept` is read back (the
+// one synchronisation of this step).
 static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int nsel, int* kept) {
   cd* V = ctx->dv_V.as<cd>();
-  cd* tblk = V + (long long)m * N;
-  cd* C = ctx->dv_G.as<cd>();
-  const int ldC = DAV_MAX_BASIS;
-  for (int pass = 0; pass < 2; pass++) {
-    if (m > 0) {
-      XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nsel, (int)N, &kOne, V, (int)N, tblk, (int)N, &kZero, C, ldC));
-      XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nsel, m, &kMinusOne, V, (int)N, C, ldC, &kOne, tblk,
-                     (int)N));
-    }
+  cd* t = V + (long long)m * N;
+  cd* X = ctx->dv_tmp.as<cd>();
+  cd* Z = ctx->dv_G.as<cd>();
+  const int ldZ = DAV_MAX_BASIS;
+  cd* S = Z + (size_t)DAV_MAX_BASIS * DAV_MAX_BASIS / 2;   // nsel x nsel (nsel <= DAV_MAX_BASIS / 2)
+  int* dkept = reinterpret_cast<int*>(ctx->dv_norm.as<double>() + 1024);
+  if (m > 0) {
+    XATU_TRY(ts_proj(ctx, V, m, t, nsel, N, Z, ldZ));
+    XATU_TRY(ts_update(ctx, t, nsel, V, m, Z, ldZ, nullptr, t, N));
   }
-  int cur = nsel;
-  for (int pass = 0; pass < 2 && cur > 0; pass++) {
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, cur, cur, (int)N, &kOne, tblk, (int)N, tblk, (int)N, &kZero, C, ldC));
-    std::vector<Z> Gh((size_t)cur * cur), Gc((size_t)ldC * cur);
-    XATU_CK(cudaMemcpyAsync(Gc.data(), C, sizeof(Z) * (size_t)ldC * cur, cudaMemcpyDeviceToHost, ctx->stream));
-    XATU_CK(cudaStreamSynchronize(ctx->stream));
-    for (int c = 0; c < cur; c++)
-      for (int r = 0; r < cur; r++) Gh[r + (size_t)c * cur] = Gc[r + (size_t)c * ldC];
-    std::vector<Z> S;
-    const int k = gram_to_orthonormalizer(Gh, cur, pass == 0 ? 1e-20 : 1e-24, S);
-    if (k == 0) {
-      cur = 0;
-      break;
-    }
-    // tmp = tblk * S  (N x k), then copy back into tblk
-    XATU_CK(ctx->dv_small.ensure(sizeof(Z) * (size_t)cur * k + 64));
-    XATU_CK(cudaMemcpyAsync(ctx->dv_small.p, S.data(), sizeof(Z) * (size_t)cur * k, cudaMemcpyHostToDevice, ctx->stream));
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, k, cur, &kOne, tblk, (int)N, ctx->dv_small.as<cd>(), cur,
-                   &kZero, ctx->dv_tmp.as<cd>(), (int)N));
-    XATU_CK(cudaMemcpyAsync(tblk, ctx->dv_tmp.p, sizeof(cd) * (size_t)N * k, cudaMemcpyDeviceToDevice, ctx->stream));
-    cur = k;
-  }
-  *kept = cur;
+  XATU_TRY(ts_proj(ctx, V, m + nsel, t, nsel, N, Z, ldZ));
+  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(nsel), ctx->stream>>>(Z, ldZ, m, nsel, 1e-20, S, dkept);
+  ctx->launches++;
+  XATU_CK_LAUNCH("ts_gram_orth_kernel");
+  XATU_TRY(ts_update(ctx, t, nsel, m > 0 ? V : nullptr, m, Z, ldZ, S, X, N));
+  XATU_TRY(ts_proj(ctx, X, nsel, X, nsel, N, Z, ldZ));
+  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(nsel), ctx->stream>>>(Z, ldZ, 0, nsel, 1e-24, S, dkept);
+  ctx->launches++;
+  XATU_CK_LAUNCH("ts_gram_orth_kernel");
+  XATU_TRY(ts_update(ctx, X, nsel, nullptr, 0, nullptr, 0, S, t, N));
+  XATU_CK(cudaMemcpyAsync(ctx->h_small, dkept, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  XATU_CK(cudaStreamSynchronize(ctx->stream));
+  *kept = *reinterpret_cast<int*>(ctx->h_small);
   return XATU_OK;
 }
 
@@ -404,6 +337,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   XATU_CK(ctx->dv_V.ensure(vbytes));
   XATU_CK(ctx->dv_W.ensure(vbytes));
   XATU_CK(ctx->dv_R.ensure((size_t)N * bsz * sizeof(cd)));
+  if (!ctx->h_small) XATU_CK(cudaMallocHost(&ctx->h_small, 8192));
   XATU_CK(ctx->dv_U.ensure((size_t)2 * N * bsz * sizeof(cd)));
   XATU_CK(ctx->dv_tmp.ensure((size_t)N * mmax * sizeof(cd)));
   XATU_CK(ctx->dv_T.ensure((size_t)DAV_MAX_BASIS * DAV_MAX_BASIS * sizeof(cd) * 3 + 4096));
@@ -412,7 +346,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   XATU_CK(ctx->dv_norm.ensure(4096 * sizeof(double)));
   cd* V = ctx->dv_V.as<cd>();
   cd* W = ctx->dv_W.as<cd>();
-  cd* R = ctx->dv_R.as<cd>();
+  cd* P = ctx->dv_R.as<cd>();                           // preconditioned residuals (N x bsz)
   cd* U = ctx->dv_U.as<cd>();                           // Ritz vectors V Y (N x bsz)
   cd* WU = U + (size_t)N * bsz;                         // W Y
   const int ldT = DAV_MAX_BASIS;
@@ -451,6 +385,13 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(cudaGetLastError());
   }
   XATU_CK(xatu_raise_smem_limit((const void*)dav_heev_kernel, heev_smem_bytes(DAV_MAX_BASIS, DAV_MAX_BASIS / 2)));
+  {
+    const int bmax = DAV_MAX_BASIS / 2;
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_proj_kernel, 224 * 1024));
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_update_kernel, 224 * 1024));
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_ritz_kernel, 224 * 1024));
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_gram_orth_kernel, ts_gram_orth_smem(bmax)));
+  }
 
   // Thick-restart block Davidson on the basis V (W = H V):
   //   T[:, new] = V^H W[:, new] (the old block of T is kept);  lowest nritz Ritz pairs of T;
@@ -472,8 +413,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     // 1. W for the new columns
     XATU_TRY(xatu_apply_h(ctx, N, m0, nnew));
     // 2. new columns of T = V^H W
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_C, CUBLAS_OP_N, m, nnew, (int)N, &kOne, V, (int)N, W + (long long)m0 * N, (int)N,
-                   &kZero, T + (long long)m0 * ldT, ldT));
+    XATU_TRY(ts_proj(ctx, V, m, W + (long long)m0 * N, nnew, N, T + (long long)m0 * ldT, ldT));
     {
       const int tot = nnew * m;
       dav_hermitize_kernel<<<(tot + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, m0);
@@ -487,17 +427,31 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     ctx->launches++;
     XATU_CK(cudaGetLastError());
     // 4. Ritz vectors and residuals
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, V, (int)N, Yr, ldT, &kZero, U, (int)N));
-    XATU_TRY(zgemm(ctx, CUBLAS_OP_N, CUBLAS_OP_N, (int)N, nritz, m, &kOne, W, (int)N, Yr, ldT, &kZero, WU, (int)N));
-    dav_residual_kernel<<<nritz, 512, 0, ctx->stream>>>(U, WU, theta, N, R, norms);
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
-    XATU_CK(cudaMemcpyAsync(h_theta.data(), theta, nritz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    XATU_CK(cudaMemcpyAsync(h_norm.data(), norms, nritz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    int st = 0;
-    XATU_CK(cudaMemcpyAsync(&st, ctx->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    {
+      const int TR = ts_ritz_smem(m, nritz, 64) <= 100 * 1024 ? 64 : 32;
+      const int G = (int)((N + TR - 1) / TR);
+      XATU_TRY(ts_part_ensure(ctx, (size_t)G * nritz * sizeof(cd)));
+      ts_ritz_kernel<<<G, TS_THREADS, ts_ritz_smem(m, nritz, TR), ctx->stream>>>(
+          V, W, m, Yr, ldT, nritz, theta, diagH, N, TR, U, WU, P, ctx->dv_part.as<cd>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("ts_ritz_kernel");
+      // squared residual norms as complex pairs at [256, 256 + 2 nritz), the status word at 768
+      ts_sum_kernel<<<(nritz + 31) / 32, TS_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, nritz, nritz,
+                                                                         reinterpret_cast<cd*>(norms), 1,
+                                                                         ctx->d_status.as<int>(), theta + 768);
+      ctx->launches++;
+      XATU_CK_LAUNCH("ts_sum_kernel");
+    }
+    // one read-back: theta [0, 256), residual norms [256, 512), status word at 768
+    XATU_CK(cudaMemcpyAsync(ctx->h_small, theta, 769 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     XATU_CK(cudaStreamSynchronize(ctx->stream));
     xatu_hx_collect(ctx);
+    {
+      const double* hb = reinterpret_cast<const double*>(ctx->h_small);
+      std::copy(hb, hb + nritz, h_theta.begin());
+      for (int c = 0; c < nritz; c++) h_norm[c] = std::sqrt(hb[256 + 2 * c]);
+    }
+    const int st = (int)reinterpret_cast<const double*>(ctx->h_small)[768];
     if (st) {
       cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream);
       return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz or K.X stage reported an error");
@@ -534,10 +488,10 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(cudaMemcpyAsync(sel_dev, sel.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     {
       const long long tot = N * nsel;
-      dav_precondition_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(
-          R, theta, diagH, sel_dev, nsel, N, V, m);
+      ts_gather_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(P, sel_dev, nsel, N,
+                                                                                          V + (long long)m * N);
       ctx->launches++;
-      XATU_CK(cudaGetLastError());
+      XATU_CK_LAUNCH("ts_gather_kernel");
     }
     int kept = 0;
     XATU_TRY(orthonormalize_block(ctx, N, m, nsel, &kept));

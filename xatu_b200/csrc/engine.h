@@ -95,6 +95,8 @@ struct xatu_ctx {
   int dav_iters = 0;
   double dav_maxres = 0;
   DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo;
+  DBuf dv_part;                // per-tile partial sums of the Davidson reductions
+  void* h_small = nullptr;     // pinned host staging for small read-backs (4 KB)
 
   // ---------------- adjoint
   bool bands_from_model = false;   // bands came from xatu_bands_compute (not uploaded)
