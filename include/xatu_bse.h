@@ -171,6 +171,12 @@ xatu_status xatu_davidson_stats(const xatu_ctx *ctx, int *iterations, double *ma
 /* Kernel of H.X for the mixed build: 0 automatic (tcgen05 tensor cores when the layout allows), 1 CUDA cores,
    2 tensor cores.  No reference counterpart (the reference multiplies dense Armadillo matrices, davidson.cpp:31-37). */
 xatu_status xatu_hx_backend(xatu_ctx *ctx, int backend);
+/* Band-solve algorithm (no counterpart in the reference, which diagonalises every H(k) in full with
+   Armadillo, SystemTB.cpp:113-125): 0 auto (band window when supported), 1 full Jacobi eigensolve of every
+   H(k), 2 eigenpairs of the band list only (Householder tridiagonalisation, Sturm multisection, inverse
+   iteration; models without overlap matrices, norb <= 64, at most 16 bands; XATU_ERR_UNSUPPORTED
+   otherwise).  Same results to rounding for bands that are not degenerate. */
+xatu_status xatu_bands_backend(xatu_ctx *ctx, int backend);
 /* Y = H X for nvec host vectors with the current build (X, Y: N x nvec complex, column-major); the product the
    Davidson iterations use. */
 xatu_status xatu_kernel_matvec(xatu_ctx *ctx, int nvec, const double *X, double *Y);

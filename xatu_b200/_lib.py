@@ -30,7 +30,7 @@ EXPORTED_SYMBOLS = [
     "xatu_system_upload", "xatu_exciton_set", "xatu_bands_compute", "xatu_bands_upload", "xatu_bands_download",
     "xatu_interaction_build", "xatu_motif_ft_download", "xatu_bse_build", "xatu_bse_dim", "xatu_bse_copy_to_host",
     "xatu_bse_device_buffers", "xatu_bse_solve", "xatu_davidson_config", "xatu_davidson_stats", "xatu_stage_times",
-    "xatu_hx_backend", "xatu_kernel_matvec", "xatu_kernel_stats", "xatu_hx_noalloc", "xatu_oscillator_strength",
+    "xatu_hx_backend", "xatu_bands_backend", "xatu_kernel_matvec", "xatu_kernel_stats", "xatu_hx_noalloc", "xatu_oscillator_strength",
     "xatu_bse_build_basis", "xatu_adjoint", "xatu_oscillator_window_gradient", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
     "xatu_batch_set_stream", "xatu_batch_add", "xatu_batch_run", "xatu_batch_dim", "xatu_batch_result",
     "xatu_batch_stats",
@@ -98,6 +98,7 @@ def lib() -> ctypes.CDLL:
         "xatu_davidson_stats": ([vp, ctypes.POINTER(ci), ctypes.POINTER(cd_)], ci),
         "xatu_stage_times": ([vp, ctypes.POINTER(ctypes.c_float)], ci),
         "xatu_hx_backend": ([vp, ci], ci),
+        "xatu_bands_backend": ([vp, ci], ci),
         "xatu_kernel_matvec": ([vp, ci, vp, vp], ci),
         "xatu_kernel_stats": ([vp, ci, i64p, ctypes.POINTER(cd_), ctypes.POINTER(ci)], ci),
         "xatu_hx_noalloc": ([vp, vp, vp, ctypes.c_int64, ctypes.c_int64, ci, vp, vp, vp], ci),

@@ -362,6 +362,31 @@ xatu_status xatu_bands_enqueue(xatu_ctx* ctx) {
   bp.max_sweeps = 40;
   bp.has_overlap = ctx->has_overlap ? 1 : 0;
   bp.is_au = ctx->is_au ? 1 : 0;
+  const bool window = ctx->band_backend != 1 && xatu_band_select_supported(bp.norb, bp.nb, bp.has_overlap);
+  if (ctx->band_backend == 2 && !window)
+    return xatu_fail(ctx, XATU_ERR_UNSUPPORTED, "band-window solve: needs no overlap, norb <= 64, <= 16 bands");
+  ctx->band_last_path = window ? 2 : 1;
+  if (window) {
+    cudaError_t e = xatu_launch_band_select(bp, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(),
+                                            ctx->d_HR.as<cd>(), ctx->d_eigval.as<double>(), ctx->d_eigvec.as<cd>(),
+                                            ctx->d_status.as<int>(), ctx->stream);
+    if (e != cudaSuccess) return xatu_cuda_fail(ctx, e, "launch of band_select_kernel");
+    ctx->launches++;
+    if (ctx->qnonzero) {
+      for (int i = 0; i < 3; i++) bp.shift[i] = ctx->Q[i];
+      e = xatu_launch_band_select(bp, ctx->d_kpoints.as<double>(), ctx->d_cellsR.as<double>(), ctx->d_HR.as<cd>(),
+                                  ctx->d_eigvalQ.as<double>(), ctx->d_eigvecQ.as<cd>(), ctx->d_status.as<int>(),
+                                  ctx->stream);
+      if (e != cudaSuccess) return xatu_cuda_fail(ctx, e, "launch of band_select_kernel (k+Q)");
+      ctx->launches++;
+    } else {
+      XATU_CK(cudaMemcpyAsync(ctx->d_eigvalQ.p, ctx->d_eigval.p, nk * nb * sizeof(double), cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+      XATU_CK(cudaMemcpyAsync(ctx->d_eigvecQ.p, ctx->d_eigvec.p, nk * nb * norb * sizeof(cd),
+                              cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return XATU_OK;
+  }
   const size_t smem = band_solve_smem(ctx->norb, ctx->nR, bp.has_overlap);
   XATU_CK(xatu_raise_smem_limit((const void*)band_solve_kernel, smem));
   const int grid = ctx->nk, threads = 128;
@@ -790,6 +815,13 @@ xatu_status xatu_davidson_config(xatu_ctx* ctx, double tol, int max_iter, int bl
   ctx->dav_tol = tol;
   ctx->dav_max_iter = max_iter > 0 ? max_iter : 1000;
   ctx->dav_block = block;
+  return XATU_OK;
+}
+
+xatu_status xatu_bands_backend(xatu_ctx* ctx, int backend) {
+  if (!ctx) return XATU_ERR_INVALID;
+  if (backend < 0 || backend > 2) return xatu_fail(ctx, XATU_ERR_INVALID, "backend must be 0, 1 or 2");
+  ctx->band_backend = backend;
   return XATU_OK;
 }
 

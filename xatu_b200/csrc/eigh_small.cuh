@@ -134,7 +134,7 @@ __device__ __forceinline__ int heev_poff(int r, int m) { return r * (m - 1) - r 
 // eigenvectors.  refl: global scratch of m * m complex.  prof (may be NULL):
 // clock64() at the 8 phase boundaries.  Every thread of the CTA calls this
 // (blockDim.x == HEEV_THREADS).
-__device__ void heev_lowest(const cd* __restrict__ Tg, int ldt, int m, int k, double* __restrict__ theta,
+static __device__ void heev_lowest(const cd* __restrict__ Tg, int ldt, int m, int k, double* __restrict__ theta,
                             cd* __restrict__ Yg, int ldy, cd* __restrict__ refl, unsigned char* smem,
                             int* __restrict__ status, long long* __restrict__ prof = nullptr) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

@@ -87,6 +87,8 @@ struct xatu_ctx {
   int dav_max_iter = 1000;
   int dav_block = 0;
   int hx_backend = 0;         // 0 auto, 1 CUDA cores, 2 tensor cores (tcgen05)
+  int band_backend = 0;       // 0 auto, 1 full band solve (Jacobi), 2 band window only
+  int band_last_path = -1;    // path of the last band solve (1 full, 2 window)
   long long hx_calls = 0;     // K.X launches of the last solve
   double hx_ms = 0;           // their summed device time
   int hx_last_path = -1;      // 1 CUDA cores, 2 tcgen05

@@ -15,6 +15,11 @@ extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb
 extern "C" __global__ void band_solve_kernel(BandParams bp, const double* kpoints, const double* cellsR, const cd* HR,
                                              const cd* SR, double* eigval, cd* eigvec, int* status);
 extern "C" size_t band_solve_smem(int norb, int nR, int has_overlap);
+// Band-window solve (bands_select.cu): eigenpairs of the band list only, models without overlap.
+extern "C" bool xatu_band_select_supported(int norb, int nb, int has_overlap);
+extern "C" cudaError_t xatu_launch_band_select(const BandParams& bp, const double* kpoints, const double* cellsR,
+                                               const cd* HR, double* eigval, cd* eigvec, int* status,
+                                               cudaStream_t s);
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path);
 

@@ -410,6 +410,10 @@ class ExcitonTB:
         """K.X kernel of the mixed build: "auto", "cuda" (CUDA cores) or "tc" (tcgen05 tensor cores)."""
         self._call("xatu_hx_backend", {"auto": 0, "cuda": 1, "tc": 2}[backend])
 
+    def setBandsBackend(self, backend: str):
+        """Band solve: "auto", "full" (every eigenpair of H(k), Jacobi) or "window" (the band list only)."""
+        self._call("xatu_bands_backend", {"auto": 0, "full": 1, "window": 2}[backend])
+
     def matvec(self, X: np.ndarray) -> np.ndarray:
         """H X on the device with the current build (X: N x nvec complex)."""
         X = np.asarray(X, dtype=np.complex128)
