@@ -34,7 +34,7 @@ bse_assemble_batch_kernel(const AsmBatchMember* __restrict__ members, const int2
 
 size_t xatu_assembly_batch_smem(int nv, int nc, int na, int tk, int norb, int exchange) {
   const int tr = tk * nv * nc;
-  return (2 * (size_t)(nv + nc) * norb * tk + (size_t)tr * (tr + 1) + (exchange ? 2 * (size_t)tr * na : 0)) *
+  return (2 * (size_t)(nv + nc) * norb * (tk + 1) + (size_t)tr * (tr + 1) + (exchange ? 2 * (size_t)tr * na : 0)) *
          sizeof(cplx<float>);
 }
 

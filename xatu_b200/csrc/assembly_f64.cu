@@ -15,7 +15,7 @@ static cudaError_t launch_tile(const AsmParams& p, const AsmInputs& in, const As
   const int nblk = (p.nk + TK - 1) / TK;
   const int ntiles = nblk * (nblk + 1) / 2;
   constexpr int TR = TK * NV * NC;
-  const size_t smem = (2 * (size_t)(NV + NC) * p.norb * TK + (size_t)TR * (TR + 1) +
+  const size_t smem = (2 * (size_t)(NV + NC) * p.norb * (TK + 1) + (size_t)TR * (TR + 1) +
                        (p.exchange ? 2 * (size_t)TR * NA : 0)) *
                       sizeof(cplx<T>);
   if (smem > 200 * 1024) return cudaErrorNotSupported;

@@ -71,18 +71,24 @@ __device__ __forceinline__ void write_element(const AsmParams& p, const AsmOutpu
 }
 
 // Tiles: blockIdx.x enumerates the upper-triangular k-block pairs (kb <= kb2).
+// Row r of the enumeration starts at S(r) = r nblk - r (r - 1) / 2: r from the quadratic formula, then an
+// exact correction.
 __device__ __forceinline__ void tile_of(int t, int nblk, int& kb, int& kb2) {
-  // row kb holds nblk - kb tiles
-  int r = 0, rem = t;
-  while (rem >= nblk - r) { rem -= nblk - r; r++; }
+  const double b = 2.0 * nblk + 1.0;
+  int r = (int)floor(0.5 * (b - sqrt(fmax(b * b - 8.0 * t, 0.0))));
+  r = max(0, min(r, nblk - 1));
+  auto S = [nblk](int q) { return q * nblk - q * (q - 1) / 2; };
+  while (r > 0 && S(r) > t) r--;
+  while (r + 1 < nblk && S(r + 1) <= t) r++;
   kb = r;
-  kb2 = r + rem;
+  kb2 = r + (t - S(r));
 }
 
 // Fast-path kernel.  CTA = a TK x TK tile of (k, k') pairs (TK = 16), one thread
 // per pair.
-//   phase 1: band coefficients of both k blocks (and the exchange factors of the
-//            tile's rows and columns) are staged in shared memory;
+//   phase 1: band coefficients of both k blocks (read as contiguous per-k rows,
+//            stored transposed with padded rows) and the exchange factors of the
+//            tile's rows and columns are staged in shared memory;
 //   phase 2: each thread forms T_a(v', v) = sum_b V_ab rho2_b(v', v), then for
 //            every (c, c') the conduction factors rho1_a(c, c'), and writes the
 //            final matrix values of its NC*NV x NC*NV block into a shared-memory
@@ -102,7 +108,8 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
   int kb, kb2;
   tile_of(tile, nblk, kb, kb2);
   const int norb = p.norb;
-  const int side_sz = NB * norb * TK;
+  constexpr int TKP = TK + 1;      // padded coefficient row (bank-conflict-free transposed stores)
+  const int side_sz = NB * norb * TKP;
   E* sC = reinterpret_cast<E*>(smem_raw);                  // [2][NB][norb][TK]
   E* sTile = sC + 2 * side_sz;                             // [TR][LDT]
   E* sL = sTile + TR * LDT;                                // [TR][NA] exchange rows
@@ -128,24 +135,28 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         }
     }
   }
-#pragma unroll 4
-  for (int t = tid; t < 2 * side_sz; t += blockDim.x) {
-    const int side = t / side_sz;
-    const int r = t - side * side_sz;
-    const int band = r / (norb * TK);
-    const int r2 = r - band * norb * TK;
-    const int o = r2 / TK;
-    const int kk = r2 - o * TK;
-    const int k = (side == 0 ? kb : kb2) * TK + kk;
-    E v = {T(0), T(0)};
-    if (k < p.nk) {
-      // valence bands from the k stack, conduction bands from the k+Q stack
-      const cd c = (band < NV) ? in.eigvec[((int64_t)k * p.nb + band) * norb + o]
-                               : in.eigvecQ[((int64_t)k * p.nb + band) * norb + o];
-      v.x = (T)c.x;
-      v.y = (T)c.y;
+  // coefficients: the k rows [band][orbital] are contiguous in global memory (valence part from the k
+  // stack, conduction part from the k+Q stack, same layout), so consecutive threads read consecutive
+  // elements of one k point; stored transposed, [side][band][orbital][kq] with padded rows
+  {
+    const int nbo = NB * norb;
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      const int kbase = (side == 0 ? kb : kb2) * TK;
+      E* dst = sC + side * side_sz;
+      for (int kq = 0; kq < TK; kq++) {
+        const int k = kbase + kq;
+        if (k < p.nk) {
+          const int64_t row = (int64_t)k * p.nb * norb;
+          for (int e = tid; e < nbo; e += blockDim.x) {
+            const cd c = (e < NV * norb ? in.eigvec : in.eigvecQ)[row + e];
+            dst[e * TKP + kq] = E{(T)c.x, (T)c.y};
+          }
+        } else {
+          for (int e = tid; e < nbo; e += blockDim.x) dst[e * TKP + kq] = E{T(0), T(0)};
+        }
+      }
     }
-    sC[t] = v;
   }
   const int64_t row0 = (int64_t)kb * TR, col0 = (int64_t)kb2 * TR;
   if (p.exchange) {
@@ -170,7 +181,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
   if (active) {
     const E* C1 = sC;
     const E* C2 = sC + side_sz;
-#define SCO(S, band, o, q) (S)[((band) * norb + (o)) * TK + (q)]
+#define SCO(S, band, o, q) (S)[((band) * norb + (o)) * TKP + (q)]
     // T_a(v', v) = sum_b V_ab rho2_b(v', v)
     E Tm[NA][NV][NV];
 #pragma unroll
@@ -213,18 +224,34 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
           for (int v = 0; v < NV; v++) cfma(Tm[a][v2][v], V, rho2[v2][v]);
       }
     }
+    // rho1_a(c, c') = sum_{o in a} conj(CQ_k[c]_o) CQ_k'[c']_o, each coefficient loaded once
+    E rho1a[NA][NC][NC];
+#pragma unroll
+    for (int a = 0; a < NA; a++) {
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+#pragma unroll
+        for (int c2 = 0; c2 < NC; c2++) rho1a[a][c][c2] = {T(0), T(0)};
+      for (int o = p.orb_off[a]; o < p.orb_off[a + 1]; o++) {
+        E cq[NC], cq2[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          cq[c] = SCO(C1, NV + c, o, kk);
+          cq2[c] = SCO(C2, NV + c, o, kk2);
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+#pragma unroll
+          for (int c2 = 0; c2 < NC; c2++) cfmac(rho1a[a][c][c2], cq[c], cq2[c2]);
+      }
+    }
 #pragma unroll
     for (int c = 0; c < NC; c++) {
 #pragma unroll
       for (int c2 = 0; c2 < NC; c2++) {
         E rho1[NA];
 #pragma unroll
-        for (int a = 0; a < NA; a++) {
-          E acc = {T(0), T(0)};
-          for (int o = p.orb_off[a]; o < p.orb_off[a + 1]; o++)
-            cfmac(acc, SCO(C1, NV + c, o, kk), SCO(C2, NV + c2, o, kk2));
-          rho1[a] = acc;
-        }
+        for (int a = 0; a < NA; a++) rho1[a] = rho1a[a][c][c2];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
 #pragma unroll
