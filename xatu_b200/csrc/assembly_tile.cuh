@@ -102,7 +102,11 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
   constexpr int NB = NV + NC;
   constexpr int NCV = NV * NC;
   constexpr int TR = TK * NCV;     // rows (and columns) of the staging tile
-  constexpr int LDT = TR + 1;      // padded row pitch
+  // staging tile: with TR a multiple of 16 the columns are XOR-swizzled by (row / 4) mod 16, so that the
+  // column-wise reads of the mirror block are free of bank conflicts; otherwise rows are padded by one
+  constexpr bool SWZ = (TR % 16) == 0;
+  constexpr int LDT = SWZ ? TR : TR + 1;   // row pitch
+#define TIDX(r, c) ((r) * LDT + (SWZ ? ((c) ^ (((r) >> 2) & 15)) : (c)))
   using E = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int kb, kb2;
@@ -288,7 +292,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
               val.x = -d.x;
               val.y = -d.y;
             }
-            sTile[r * LDT + cc] = val;
+            sTile[TIDX(r, cc)] = val;
           }
         }
       }
@@ -303,8 +307,8 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
     for (int t = tid; t < TR * TR; t += blockDim.x) {
       const int r = t / TR, c = t - r * TR;
       if (r > c && r < rows) {
-        const E u = sTile[c * LDT + r];
-        sTile[r * LDT + c] = E{u.x, -u.y};
+        const E u = sTile[TIDX(c, r)];
+        sTile[TIDX(r, c)] = E{u.x, -u.y};
       }
     }
     __syncthreads();
@@ -321,7 +325,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         __align__(16) __nv_bfloat162 h[VEC], l[VEC];
 #pragma unroll
         for (int q = 0; q < VEC; q++) {
-          const E v = sTile[r * LDT + c + q];
+          const E v = sTile[TIDX(r, c + q)];
           const float re = (float)v.x, im = (float)v.y;
           const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
           h[q].x = hr;
@@ -333,7 +337,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
       } else {
         for (int q = 0; q < VEC && c + q < cols; q++) {
-          const E v = sTile[r * LDT + c + q];
+          const E v = sTile[TIDX(r, c + q)];
           split_store(out.Khi, out.Klo, o + q, (float)v.x, (float)v.y);
         }
       }
@@ -349,7 +353,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
           __align__(16) __nv_bfloat162 h[VEC], l[VEC];
 #pragma unroll
           for (int q = 0; q < VEC; q++) {
-            const E v = sTile[(r + q) * LDT + c];
+            const E v = sTile[TIDX(r + q, c)];
             const float re = (float)v.x, im = -(float)v.y;
             const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
             h[q].x = hr;
@@ -361,7 +365,7 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
           *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
         } else {
           for (int q = 0; q < VEC && r + q < rows; q++) {
-            const E v = sTile[(r + q) * LDT + c];
+            const E v = sTile[TIDX(r + q, c)];
             split_store(out.Khi, out.Klo, o + q, (float)v.x, -(float)v.y);
           }
         }
@@ -371,17 +375,18 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
     for (int t = tid; t < TR * TR; t += blockDim.x) {
       const int r = t / TR, c = t - r * TR;
       if (r >= rows || c >= cols) continue;
-      const E v = sTile[r * LDT + c];
+      const E v = sTile[TIDX(r, c)];
       out.H[(row0 + r) * p.N + col0 + c] = mk((double)v.x, (double)v.y);
     }
     if (kb != kb2) {
       for (int t = tid; t < TR * TR; t += blockDim.x) {
         const int c = t / TR, r = t - c * TR;
         if (r >= rows || c >= cols) continue;
-        const E v = sTile[r * LDT + c];
+        const E v = sTile[TIDX(r, c)];
         out.H[(col0 + c) * p.N + row0 + r] = mk((double)v.x, -(double)v.y);
       }
     }
   }
+#undef TIDX
 }
 
