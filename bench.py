@@ -501,6 +501,10 @@ def run_engine(args):
     #  * K.X product: reads K (8 B per element), the BF16 operand planes (2 x 2b x 2N x 2 B)
     #    and adds into Y (N x 2b FP32).
     hbm, bf16, src = peaks()
+    # DRAM traffic of the K.X product per launch, from an ncu capture of the same kernel at N = 5184
+    # (k mesh 36 x 36, K = 215 MB > L2; dram__bytes_read.sum + dram__bytes_write.sum = 220.4 MB per launch,
+    # profiles/hx_tcgen05_traffic.md), scaled by N^2 (the reads stream K once, so traffic grows with it)
+    hx_traffic_per_element = (219.78e6 + 0.61e6) / 5184.0 ** 2
     asm_s = statistics.median(asm_ms) / 1e3
     asm_bytes = N * N * 8 + N * 8
     kernels = [{"kernel": "bse_assemble_tile_kernel<float,2,2,3,mixed>", "bound": "hbm",
@@ -514,7 +518,8 @@ def run_engine(args):
         hx_bytes = N * N * 8 + 2 * ng * 2 * N * 2 + N * ng * 4
         kernels.append({"kernel": "hx_tcgen05_kernel" if hx_path == 2 else "hx_cuda_core_kernel", "bound": "hbm",
                         "achieved": hx_bytes / hx_s / 1e9, "peak": hbm, "unit": "GB/s",
-                        "frac": hx_bytes / hx_s / 1e9 / hbm, "peak_source": src, "traffic": None,
+                        "frac": hx_bytes / hx_s / 1e9 / hbm, "peak_source": src,
+                        "traffic": hx_traffic_per_element * N * N if hx_path == 2 else None,
                         "algorithmic_bytes_per_launch": hx_bytes, "launch_ms": hx_s * 1e3,
                         "launches_per_step": calls / len(hx_n)})
     roofline = max(kernels, key=lambda k: k["launch_ms"] * k["launches_per_step"])
