@@ -189,6 +189,54 @@ xatu_status xatu_kernel_matvec(xatu_ctx *ctx, int nvec, const double *X, double 
    modified in place. */
 xatu_status xatu_oscillator_strength(xatu_ctx *ctx, int nstates, const double *eigvec, double *vme_ex);
 
+/* ------------------------------------------------------------------ post-processing of exciton states */
+/* The observables and writers of Result / ResultTB evaluated on the device for a batch of states.  eigvec is
+   host, N x nstates complex, column-major, in the full e-h basis of the context (row k*nc*nv + c*nv + v); the
+   band stacks are the context's (computed or uploaded).  XATU_ERR_UNSUPPORTED when the last build used a
+   caller-given basis subset. */
+
+/* Per-state reductions, each output optional (NULL skips it):
+     kinetic[s]       Result::kineticEnergy (Result.tpp:25-40): sum |A|^2 (E^Q_c(k) - E_v(k)), no scissor;
+     kweight[s*nk+k]  sum_{c,v} |A(k,c,v)|^2, the numerator of writeReciprocalAmplitude / ftExcitonEnvelope
+                      (Result.tpp:101-128, :160-226);
+     peak[s]          Result::findExcitonPeak (Result.tpp:478-484): k index of the first largest |A|;
+     spin[6*s ..]     ResultTB::spinX (ResultTB.cpp:21-98) as three complex numbers {total, hole, electron};
+                      XATU_ERR_INVALID when an atom has an odd number of orbitals (the reference throws). */
+xatu_status xatu_state_observables(xatu_ctx *ctx, int nstates, const double *eigvec, double *kinetic,
+                                   double *kweight, int64_t *peak, double *spin);
+
+/* ResultTB::realSpaceWavefunction (ResultTB.cpp:310-357) for every state, electron cell and electron atom:
+   out[(s*ncells + cell)*natoms + atom] = sum over the orbitals a of `atom` and b of atom hole_index of
+   |sum_{k,c,v} C^Q_{k,c}[a] conj(C_{k,v}[b]) A_s(k,c,v) exp(i k.(cells[cell] - hole_cell))|^2 -- the loop of
+   writeRealspaceAmplitude (ResultTB.cpp:370-408).  cells: ncells x 3 (Angstrom); hole_cell: 3. */
+xatu_status xatu_realspace_amplitude(xatu_ctx *ctx, int nstates, const double *eigvec, int hole_index,
+                                     const double *hole_cell, int ncells, const double *cells, double *out);
+
+/* Result::ftExcitonEnvelope (Result.tpp:101-128) at npoints separations d = r_e - r_h (npoints x 3):
+   out[s*npoints + p] = Re sum_k kweight_s(k) exp(-i k.d_p). */
+xatu_status xatu_envelope_ft(xatu_ctx *ctx, int nstates, const double *eigvec, int npoints, const double *points,
+                             double *out);
+
+/* Broadening of the exciton peaks in skubo_w's broad_vector (skubo_w.f90:684-720); any other value keeps the
+   reference's default weight 1. */
+enum {
+  XATU_BROAD_OTHER = 0,
+  XATU_BROAD_LORENTZIAN = 1,
+  XATU_BROAD_GAUSSIAN = 2,
+  XATU_BROAD_EXPONENTIAL = 3
+};
+/* ResultTB::writeAbsorptionSpectrum -> skubo_w (ResultTB.cpp:412-461, skubo_w.f90:2-173) without the file
+   I/O: frequencies w_i = (w0 + wrange/nw * i) eV, i < nw, broadening eta (eV) -- the kubo_w.in parameters.
+     sigma_sp  nw x 9 complex: the single-particle Kubo conductivity sigma_ij(w) over every (k, c, v) with
+               the Gaussian delta of get_kubo_intens (skubo_w.f90:630-681); the file holds -Re.
+     sigma_ex  nw x 9 real: sum_n Re(pi/(nk vcell) conj(V_i,n) V_j,n / E_n) broadening(w - E_n), i, j < 2
+               (the other entries 0, as in the reference), over the nstates given states.
+     vme_ex    optional, 3 x nstates complex column-major: their velocity matrix elements (atomic units).
+   eigval: nstates exciton energies (eV).  nstates = 0 computes the single-particle part only. */
+xatu_status xatu_absorption(xatu_ctx *ctx, int nstates, const double *eigval, const double *eigvec, double w0,
+                            double wrange, int nw, double eta, int broadening, double *sigma_sp, double *sigma_ex,
+                            double *vme_ex);
+
 /* ------------------------------------------------------------------ adjoint gradients */
 #define XATU_ADJOINT_MAX_STATES 8
 /* Hellmann-Feynman gradients dE_n/dtheta = x_n^H (dH/dtheta) x_n of exciton energies through the whole path

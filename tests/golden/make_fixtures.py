@@ -52,6 +52,13 @@ HASHES = {
                 "hash": 1.086145105, "tol": 1e-5},
     "MoS2_kwf": {"model": "MoS2.model", "ncell": 12, "nbands": 2, "params": [1., 4., 13.55], "nstates": 2,
                  "hash": 1.1814790902, "tol": 1e-5},
+    # tests.cpp:323-369 (real-space wavefunction hash: hole on atom 1 of cell 0, electron cells within
+    # |a1| * ncell, summed over the lowest 2 states)
+    "hBN_rswf": {"model": "hBN.model", "ncell": 20, "nbands": 1, "params": [1, 1, 10], "nstates": 2,
+                 "hole_index": 1, "hole_cell": [0, 0, 0], "radius_cells": 20, "hash": 3.4185866144, "tol": 1e-5},
+    # tests.cpp:432-462 (spinX of the lowest 4 states of spinful hBN: total Sz, |hole| = |electron| = 1/2)
+    "hBN_spin": {"model": "hBN_spinful.model", "ncell": 16, "nbands": 2, "params": [1, 1, 10], "nstates": 4,
+                 "total": [-1, 0, 0, 1], "abs_parts": 0.5, "tol": 1e-2},
 }
 
 
@@ -61,12 +68,14 @@ def _check_against_tests(ref: str):
         for e, d in case[8]:
             if f"{e:.6f}" not in text:
                 raise SystemExit(f"{case[0]}: {e:.6f} not found in tests.cpp")
-    for key in ("hBN_kwf", "MoS2_kwf"):
+    for key in ("hBN_kwf", "MoS2_kwf", "hBN_rswf"):
         if repr(HASHES[key]["hash"]) not in text:
             raise SystemExit(f"{key}: hash not found in tests.cpp")
     for v in ("4.55422", "3.90211", "-0.110843", "-1.34375", "-0.0375"):
         if v not in text:
             raise SystemExit(f"parse hash {v} not found")
+    if "arma::vec{-1, 0, 0, 1}" not in text or "WithinAbs(0.5, 1E-2)" not in text:
+        raise SystemExit("spin golden not found")
     if not re.search(r"expectedName = \"hBN_N30\"", text):
         raise SystemExit("exciton parse golden not found")
 

@@ -1,0 +1,279 @@
+"""Device post-processing (xatu_state_observables, xatu_realspace_amplitude, xatu_envelope_ft,
+xatu_absorption and the ResultTB writers) against the oracle's restatement of Result.tpp / ResultTB.cpp /
+skubo_w.f90 and against the reference's goldens.
+
+Parity runs with the oracle's band stacks uploaded to the engine, so both sides see the same band gauge and
+the same exciton coefficients; the bars are relative 1e-10 for the transforms and sums (FP64 with a different
+summation order).  The golden tests run the whole device path (bands, FP64 build, dense solve)."""
+import io
+
+import numpy as np
+import pytest
+
+from oracle.oracle import array2hash, truncate_supercell
+from oracle import postproc as PP
+from tests.helpers import engine_exciton, goldens, model_config, oracle_exciton
+from xatu_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-10
+
+
+def _shared(model, ncell, nbands, params, nstates=6, **kw):
+    """Engine and oracle on the same bands; the oracle's lowest eigenvectors."""
+    cfg = model_config(model)
+    ex = engine_exciton(cfg, ncell, nbands, params, **kw)
+    orc = oracle_exciton(cfg, ncell, nbands, params, **kw)
+    ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
+    w, v = np.linalg.eigh(orc.bs_hamiltonian())
+    from xatu_b200.result import ResultTB
+    return ex, orc, ResultTB(ex, w[:nstates], v[:, :nstates].copy()), w, v
+
+
+PARITY = [
+    ("hBN", "hBN.model", 12, 1, [1, 1, 10], {}),
+    ("MoS2_Q", "MoS2.model", 9, 2, [1., 4., 13.55], {"Q": (0, 0.05, 0)}),
+    ("hBN_spinful", "hBN_spinful.model", 10, 2, [1, 1, 10], {}),
+]
+
+
+@pytest.mark.parametrize("name,model,ncell,nbands,params,kw", PARITY, ids=[c[0] for c in PARITY])
+def test_state_observables_match_oracle(name, model, ncell, nbands, params, kw):
+    ex, orc, res, w, v = _shared(model, ncell, nbands, params, **kw)
+    spin = name == "hBN_spinful"
+    obs = res.observables(spin=spin)
+    nbc = len(orc.valence) * len(orc.conduction)
+    for s in range(res.eigvec.shape[1]):
+        x = res.eigvec[:, s]
+        assert obs["kinetic"][s] == pytest.approx(PP.kinetic_energy(orc, x), rel=1e-12, abs=1e-12)
+        assert np.abs(obs["kweight"][s] - PP.reciprocal_weights(orc, x)).max() < 1e-13
+        # first largest |A|: the device's k block holds a coefficient equal to the maximum
+        amax = np.abs(x).max()
+        blk = np.abs(x[obs["peak"][s] * nbc:(obs["peak"][s] + 1) * nbc]).max()
+        assert blk >= amax * (1 - 1e-13)
+        if blk == amax and np.sum(np.abs(x) >= amax * (1 - 1e-13)) == 1:
+            assert obs["peak"][s] == PP.find_exciton_peak(orc, x)
+        if spin:
+            ref = PP.spin_x(orc, x)
+            assert np.abs(obs["spin"][s] - ref).max() < 1e-12
+        assert res.potentialEnergy(s) == pytest.approx(w[s] - PP.kinetic_energy(orc, x), abs=1e-11)
+
+
+@pytest.mark.parametrize("name,model,ncell,nbands,params,kw", PARITY, ids=[c[0] for c in PARITY])
+def test_realspace_amplitude_matches_oracle(name, model, ncell, nbands, params, kw):
+    ex, orc, res, w, v = _shared(model, ncell, nbands, params, nstates=3, **kw)
+    s = orc.system
+    cells = truncate_supercell(s.bravais, s.ndim, ncell, np.linalg.norm(s.bravais[0]) * 3)
+    for hole in range(s.natoms):
+        hc = np.array([1.0, 0.0, 0.0]) * (hole % 2) * np.linalg.norm(s.bravais[0])
+        dev = res.realSpaceAmplitudes(res.eigvec, hole, hc, cells)
+        for st in range(3):
+            ref = PP.realspace_amplitudes(orc, res.eigvec[:, st], hole, hc, cells)
+            assert np.abs(dev[st] - ref).max() <= REL * max(1e-30, np.abs(ref).max()), (hole, st)
+    # the single-value form of the reference
+    x = res.eigvec[:, 0]
+    a = res.realSpaceWavefunction(x, s.natoms - 1, 0, cells[1], np.zeros(3))
+    assert a == pytest.approx(PP.real_space_wavefunction(orc, x, s.natoms - 1, 0, cells[1], np.zeros(3)), rel=REL)
+
+
+@pytest.mark.parametrize("name,model,ncell,nbands,params,kw", PARITY[:2], ids=[c[0] for c in PARITY[:2]])
+def test_envelope_ft_matches_oracle(name, model, ncell, nbands, params, kw):
+    ex, orc, res, w, v = _shared(model, ncell, nbands, params, nstates=4, **kw)
+    rng = np.random.default_rng(7)
+    seps = rng.uniform(-20, 20, size=(37, 3))
+    seps[:, 2] = 0
+    seps[0] = 0
+    dev = res.ftExcitonEnvelopes(res.eigvec, seps)
+    for st in range(4):
+        ref = np.array([PP.ft_exciton_envelope(orc, res.eigvec[:, st], d, np.zeros(3)) for d in seps])
+        assert np.abs(dev[st] - ref).max() < 1e-12
+    assert res.ftExcitonEnvelope(0, seps[3] + 1.0, np.ones(3)) == pytest.approx(dev[0, 3], abs=1e-13)
+
+
+@pytest.mark.parametrize("name,model,ncell,nbands,params,kw", PARITY[:2], ids=[c[0] for c in PARITY[:2]])
+@pytest.mark.parametrize("kind", ["lorentzian", "gaussian", "exponential", "other"])
+def test_absorption_matches_oracle(name, model, ncell, nbands, params, kw, kind):
+    ex, orc, res, w, v = _shared(model, ncell, nbands, params, nstates=8, **kw)
+    w0, wrange, nw, eta = 1.0, 6.0, 60, 0.08
+    r = res.absorptionSpectrum(w0, wrange, nw, eta, kind)
+    if kind == "lorentzian":   # the single-particle part does not depend on the kind
+        sp = PP.kubo_single_particle(orc, w0, wrange, nw, eta)
+        assert np.abs(r["sigma_sp"] - sp).max() <= REL * np.abs(sp).max()
+    sx, vx = PP.exciton_absorption(orc, w[:8], v[:, :8], w0, wrange, nw, eta, kind)
+    assert np.abs(r["sigma_ex"] - sx).max() <= REL * np.abs(sx).max()
+    assert np.abs(r["vme_ex"] - vx).max() <= 1e-9 * np.abs(vx).max()
+    assert np.allclose(r["w"], PP.frequencies(w0, wrange, nw) * 27.211385, rtol=1e-15, atol=0)
+
+
+def test_absorption_single_particle_only():
+    ex, orc, res, w, v = _shared("hBN.model", 8, 1, [1, 1, 10])
+    from xatu_b200.result import ResultTB
+    empty = ResultTB(ex, np.zeros(0), None)
+    r = empty.absorptionSpectrum(2.0, 8.0, 40, 0.1)
+    sp = PP.kubo_single_particle(orc, 2.0, 8.0, 40, 0.1)
+    assert np.abs(r["sigma_sp"] - sp).max() <= REL * np.abs(sp).max()
+    assert np.all(r["sigma_ex"] == 0)
+
+
+# ------------------------------------------------------------------ the reference's goldens, device path
+
+
+def _device_solved(g, nstates, precision="fp64", method="diag"):
+    ex = engine_exciton(model_config(g["model"]), g["ncell"], g["nbands"], g["params"])
+    ex.BShamiltonian(precision)
+    return ex, ex.diagonalize(method, nstates)
+
+
+def test_realspace_hash_golden_device():
+    g = goldens()["hashes"]["hBN_rswf"]
+    ex, res = _device_solved(g, g["nstates"])
+    s = ex.system
+    cells = s.truncateSupercell(g["ncell"], np.linalg.norm(s.bravaisLattice[0]) * g["radius_cells"])
+    amp = res.realSpaceAmplitudes(res.eigvec[:, :g["nstates"]], g["hole_index"], g["hole_cell"], cells)
+    rswf = amp.sum(axis=0).reshape(-1)
+    assert array2hash(rswf) == pytest.approx(g["hash"], abs=g["tol"])
+
+
+@pytest.mark.parametrize("key", ["hBN_kwf", "MoS2_kwf"])
+def test_kwf_hash_golden_device(key):
+    g = goldens()["hashes"][key]
+    ex, res = _device_solved(g, g["nstates"])
+    kp = ex.system.kpoints
+    kw = res.observables()["kweight"][:g["nstates"]].sum(axis=0) / np.linalg.norm(kp[1] - kp[0])
+    assert array2hash(kw.astype(complex)) == pytest.approx(g["hash"], abs=g["tol"])
+
+
+def test_spin_golden_device():
+    """tests.cpp:432-462.  States 1 and 2 are degenerate to ~1e-8 eV, so only their summed hole and electron
+    spins are basis independent; states 0 and 3 and every total are compared directly."""
+    g = goldens()["hashes"]["hBN_spin"]
+    ex, res = _device_solved(g, g["nstates"])
+    sp = res.observables(spin=True)["spin"]
+    for i in range(g["nstates"]):
+        assert sp[i, 0].real == pytest.approx(g["total"][i], abs=g["tol"])
+        assert res.spinX(i)[0].real == pytest.approx(g["total"][i], abs=g["tol"])
+    for i in (0, 3):
+        assert abs(sp[i, 1]) == pytest.approx(g["abs_parts"], abs=g["tol"])
+        assert abs(sp[i, 2]) == pytest.approx(g["abs_parts"], abs=g["tol"])
+    assert abs(sp[1, 1] + sp[2, 1]) < g["tol"] and abs(sp[1, 2] + sp[2, 2]) < g["tol"]
+
+
+def test_realspace_parseval_full_supercell():
+    """Size-independent property at a larger mesh: over the complete n x n supercell and every electron atom,
+    sum |G(R)|^2 = nk sum_k |A_k|^2 |C_{k,v}[hole]|^2 (one valence and one conduction band, orthonormal
+    conduction vectors) -- the discrete Parseval identity of the transform over k."""
+    cfg = model_config("hBN.model")
+    n = 48
+    ex = engine_exciton(cfg, n, 1, [1, 1, 10])
+    ex.BShamiltonian("mixed")
+    res = ex.diagonalize("davidson", 2)
+    s = ex.system
+    cells = s.truncateSupercell(n, 1e9)
+    assert cells.shape[0] == n * n
+    ev, vv, evq, vvq = ex.bandStacks()
+    kw = res.observables()["kweight"]
+    for hole in range(2):
+        amp = res.realSpaceAmplitudes(res.eigvec, hole, np.zeros(3), cells)
+        for st in range(2):
+            ref = s.nk * np.sum(kw[st] * np.abs(vv[:, 0, hole]) ** 2)
+            assert amp[st].sum() == pytest.approx(ref, rel=1e-11)
+
+
+# ------------------------------------------------------------------ writers and errors
+
+
+def test_writers_formats():
+    ex, orc, res, w, v = _shared("hBN.model", 6, 1, [1, 1, 10], nstates=3)
+    s = orc.system
+    buf = io.StringIO()
+    res.writeRealspaceAmplitude(1, 1, np.zeros(3), buf, ncells=2)
+    lines = buf.getvalue().splitlines()
+    assert lines[0] == "%11.8f\t%11.8f\t%14.11f" % (s.motif[1, 0], s.motif[1, 1], 0.0)
+    assert lines[-1] == "#"
+    cells = truncate_supercell(s.bravais, s.ndim, 6, np.linalg.norm(s.bravais[0]) * 2)
+    ref = PP.realspace_amplitudes(orc, res.eigvec[:, 1], 1, np.zeros(3), cells)
+    vals = np.array([float(l.split("\t")[2]) for l in lines[1:-1]])
+    assert len(vals) == cells.shape[0] * s.natoms
+    assert np.abs(vals - ref.reshape(-1)).max() < 1e-10
+
+    buf = io.StringIO()
+    res.writeReciprocalAmplitude(0, buf)
+    lines = buf.getvalue().splitlines()
+    assert lines[0] == "kx\tky\tkz\tProb." and lines[-1] == "#"
+    kwf = PP.reciprocal_amplitude(orc, res.eigvec[:, 0])
+    assert np.abs(np.array([float(l.split("\t")[3]) for l in lines[1:-1]]) - kwf).max() < 1e-8
+
+    buf = io.StringIO()
+    res.writeExtendedReciprocalAmplitude(0, buf)
+    box = max(orc.kpoints[:, 0].max(), orc.kpoints[:, 1].max())
+    count = 0
+    for k in orc.kpoints:
+        for i in (-1, 0, 1):
+            for j in (-1, 0, 1):
+                d = k + i * s.recip[0] + j * s.recip[1]
+                count += abs(d[0]) < box and abs(d[1]) < box
+    assert len(buf.getvalue().splitlines()) == count + 1
+
+    buf = io.StringIO()
+    res.writePhase(2, buf)
+    rows = [l.split("\t") for l in buf.getvalue().splitlines()[1:-1]]
+    x = res.eigvec[:, 2]
+    assert np.abs(np.array([float(r[3]) for r in rows]) - np.abs(x)).max() < 1e-8
+    assert np.abs(np.array([float(r[4]) for r in rows]) - np.angle(x)).max() < 1e-8
+
+    buf = io.StringIO()
+    res.writeEigenvalues(buf, 3)
+    assert buf.getvalue() == "%d\t" % res.exciton.excitonbasisdim + "".join("%11.7f\t" % e for e in w[:3]) + "\n"
+
+    buf = io.StringIO()
+    res.writeStates(buf, 2)
+    lines = buf.getvalue().splitlines()
+    N = res.exciton.excitonbasisdim
+    assert lines[0] == str(N) and len(lines) == 1 + N + 2
+    assert lines[1] == "%11.7f\t%11.7f\t%11.7f\t%d\t%d" % (orc.kpoints[0][0], orc.kpoints[0][1], orc.kpoints[0][2],
+                                                          orc.valence[0], orc.conduction[0])
+
+
+def test_write_spin_and_absorption_files(tmp_path, monkeypatch):
+    ex, orc, res, w, v = _shared("hBN_spinful.model", 8, 2, [1, 1, 10], nstates=4)
+    buf = io.StringIO()
+    res.writeSpin(4, buf)
+    lines = buf.getvalue().splitlines()
+    assert lines[0] == "n\tSt\tSe\tSh" and len(lines) == 5
+    for i, l in enumerate(lines[1:]):
+        ref = PP.spin_x(orc, res.eigvec[:, i])
+        assert l == "%d\t%11.7f\t%11.7f\t%11.7f" % (i, ref[0].real, ref[1].real, ref[2].real)
+    monkeypatch.chdir(tmp_path)
+    (tmp_path / "kubo_w.in").write_text("#w0\n1\n#range\n6\n#n\n50\n#eta\n0.08d0\n#type\ngaussian\n#files\n"
+                                        "sp.dat\nex.dat\n")
+    r = res.writeAbsorptionSpectrum()
+    sp = np.loadtxt(tmp_path / "sp.dat")
+    assert sp.shape == (50, 10)
+    assert np.abs(sp[:, 1:] + r["sigma_sp"].reshape(50, 9).real).max() <= 1e-15 * max(1, np.abs(sp).max())
+    text = (tmp_path / "ex.dat").read_text().split("\n \n")
+    ex_rows = np.loadtxt(io.StringIO(text[0]))
+    assert ex_rows.shape == (50, 10)
+    osc = np.loadtxt(io.StringIO(text[1]))
+    assert osc.shape == (4, 7)
+    assert np.allclose(osc[:, 0], w[:4], rtol=1e-14)
+
+
+def test_postproc_errors():
+    ex, orc, res, w, v = _shared("MoS2.model", 6, 2, [1., 4., 13.55], nstates=2)
+    with pytest.raises(L.XatuError) as e:
+        res.realSpaceAmplitudes(res.eigvec, 99, np.zeros(3), np.zeros((1, 3)))
+    assert e.value.status == L.XATU_ERR_INVALID
+    with pytest.raises(ValueError):
+        res.writePhase(0, io.StringIO())          # two band pairs per k
+    with pytest.raises(ValueError):
+        res.observables(np.zeros(5))              # wrong length
+    assert res.realSpaceAmplitudes(res.eigvec, 0, np.zeros(3), np.zeros((0, 3))).shape == (2, 0, orc.system.natoms)
+    ex2, orc2, res2, w2, v2 = _shared("hBN.model", 6, 1, [1, 1, 10], nstates=2)
+    with pytest.raises(L.XatuError) as e:
+        res2.spinX(0)                             # one orbital per atom (the reference throws)
+    assert e.value.status == L.XATU_ERR_INVALID
+    with pytest.raises(ValueError):
+        res2.writeEigenvalues(io.StringIO(), -1)
+    with pytest.raises(IndexError):
+        res2.writeEigenvalues(io.StringIO(), 5)   # more than stored

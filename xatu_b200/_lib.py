@@ -24,6 +24,7 @@ POT_KELDYSH, POT_COULOMB = 0, 1
 GAUGE_LATTICE, GAUGE_ATOMIC = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 SOLVER_DENSE_FP64, SOLVER_DAVIDSON = 0, 1
+BROAD_OTHER, BROAD_LORENTZIAN, BROAD_GAUSSIAN, BROAD_EXPONENTIAL = 0, 1, 2, 3
 
 EXPORTED_SYMBOLS = [
     "xatu_ctx_create", "xatu_ctx_destroy", "xatu_last_error", "xatu_ctx_set_stream", "xatu_abi_version",
@@ -31,6 +32,7 @@ EXPORTED_SYMBOLS = [
     "xatu_interaction_build", "xatu_motif_ft_download", "xatu_bse_build", "xatu_bse_dim", "xatu_bse_copy_to_host",
     "xatu_bse_device_buffers", "xatu_bse_solve", "xatu_davidson_config", "xatu_davidson_stats", "xatu_stage_times",
     "xatu_hx_backend", "xatu_bands_backend", "xatu_kernel_matvec", "xatu_kernel_stats", "xatu_hx_noalloc", "xatu_oscillator_strength",
+    "xatu_state_observables", "xatu_realspace_amplitude", "xatu_envelope_ft", "xatu_absorption",
     "xatu_bse_build_basis", "xatu_adjoint", "xatu_oscillator_window_gradient", "xatu_batch_create", "xatu_batch_destroy", "xatu_batch_last_error",
     "xatu_batch_set_stream", "xatu_batch_add", "xatu_batch_run", "xatu_batch_dim", "xatu_batch_result",
     "xatu_batch_stats",
@@ -103,6 +105,10 @@ def lib() -> ctypes.CDLL:
         "xatu_kernel_stats": ([vp, ci, i64p, ctypes.POINTER(cd_), ctypes.POINTER(ci)], ci),
         "xatu_hx_noalloc": ([vp, vp, vp, ctypes.c_int64, ctypes.c_int64, ci, vp, vp, vp], ci),
         "xatu_oscillator_strength": ([vp, ci, vp, vp], ci),
+        "xatu_state_observables": ([vp, ci, vp, vp, vp, vp, vp], ci),
+        "xatu_realspace_amplitude": ([vp, ci, vp, ci, vp, ci, vp, vp], ci),
+        "xatu_envelope_ft": ([vp, ci, vp, ci, vp, vp], ci),
+        "xatu_absorption": ([vp, ci, vp, vp, cd_, cd_, ci, cd_, ci, vp, vp, vp], ci),
         "xatu_bse_build_basis": ([vp, ci, ctypes.c_int64, vp], ci),
         "xatu_adjoint": ([vp, ci, vp, vp, vp], ci),
         "xatu_oscillator_window_gradient": ([vp, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp], ci),

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
           "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]
 SOURCES = ["api.cu", "geometry.cpp", "lattice_kernels.cu", "bands.cu", "bands_select.cu", "assembly.cu", "assembly_f32.cu", "assembly_f64.cu", "assembly_batch.cu", "dense.cu", "hx.cu",
-           "hx_tc.cu", "hx_noalloc.cu", "davidson.cu", "oscillator.cu", "adjoint.cu", "batch.cu", "osc_grad.cu"]
+           "hx_tc.cu", "hx_noalloc.cu", "davidson.cu", "oscillator.cu", "postproc.cu", "adjoint.cu", "batch.cu", "osc_grad.cu"]
 
 
 def _nvcc() -> str:

@@ -105,6 +105,9 @@ struct xatu_ctx {
   float adjoint_ms = 0;            // last xatu_adjoint call, first to last launch
   float adj_pair_ms = 0;           // its pair kernel
   DBuf d_oscG;
+
+  // ---------------- post-processing (postproc.cu)
+  DBuf d_pp_X, d_pp_A, d_pp_B, d_pp_C, d_pp_D, d_pp_P;
   DBuf d_adjX, d_adjdvtab, d_adjdtable, d_adjdVX, d_adjAlpha, d_adjExUW, d_adjCbar, d_adjEbar, d_adjEpart, d_adjGk,
       d_adjG;
 };
@@ -141,6 +144,8 @@ xatu_status xatu_dense_solve(xatu_ctx* ctx, int nstates, double* eigval, double*
 xatu_status xatu_dense_eig_device(xatu_ctx* ctx, bool vectors);
 // Velocity matrix elements of every e-h state into out (3 x N, row-major) (oscillator.cu).
 xatu_status xatu_vme_enqueue(xatu_ctx* ctx, cd* out);
+// vme_ex (3 x ns, column-major) = sum_i X(i, s) v_j(i) for the 3 x N elements v of xatu_vme_enqueue (oscillator.cu).
+xatu_status xatu_exciton_vme_enqueue(xatu_ctx* ctx, const cd* v, const cd* X, long long N, int ns, cd* out);
 // Adjoint of the velocity matrix elements (oscillator.cu): vbar (N x 3, column-major) -> added to cbar/ebar
 // and, for the direct dependence on H(R), to G (nR x norb x norb); gvme: scratch of 2 x nk x norb^2.
 // G = NULL: only cbar/ebar and gvme; xatu_vme_hop_enqueue then adds the direct part to G.

@@ -314,6 +314,13 @@ static OscParams osc_params(const xatu_ctx* ctx) {
   return p;
 }
 
+xatu_status xatu_exciton_vme_enqueue(xatu_ctx* ctx, const cd* v, const cd* X, long long N, int ns, cd* out) {
+  exciton_vme_kernel<<<3 * ns, 256, 0, ctx->stream>>>(v, X, (int)N, ns, out);
+  ctx->launches++;
+  XATU_CK_LAUNCH("exciton_vme_kernel");
+  return XATU_OK;
+}
+
 // Velocity matrix elements of every e-h state of the full basis into out (3 x N, row-major).
 xatu_status xatu_vme_enqueue(xatu_ctx* ctx, cd* out) {
   const OscParams p = osc_params(ctx);
@@ -372,10 +379,8 @@ extern "C" xatu_status xatu_oscillator_strength(xatu_ctx* ctx, int nstates, cons
   xatu_status st = xatu_vme_enqueue(ctx, ctx->dv_R.as<cd>());
   if (st != XATU_OK) return st;
   XATU_CK(cudaMemcpyAsync(ctx->dv_tmp.p, eigvec, xbytes, cudaMemcpyHostToDevice, ctx->stream));
-  exciton_vme_kernel<<<3 * nstates, 256, 0, ctx->stream>>>(ctx->dv_R.as<cd>(), ctx->dv_tmp.as<cd>(), (int)N, nstates,
-                                                           ctx->dv_small.as<cd>());
-  ctx->launches++;
-  XATU_CK(cudaGetLastError());
+  st = xatu_exciton_vme_enqueue(ctx, ctx->dv_R.as<cd>(), ctx->dv_tmp.as<cd>(), N, nstates, ctx->dv_small.as<cd>());
+  if (st != XATU_OK) return st;
   XATU_CK(cudaMemcpyAsync(vme_ex, ctx->dv_small.p, (size_t)3 * nstates * sizeof(cd), cudaMemcpyDeviceToHost,
                           ctx->stream));
   XATU_CK(cudaStreamSynchronize(ctx->stream));

@@ -22,6 +22,7 @@ import numpy as np
 
 from . import _lib as L
 from .config import ExcitonConfiguration, SystemConfiguration
+from .result import ResultTB
 
 
 class SystemTB:
@@ -77,15 +78,6 @@ class SystemTB:
 
     def truncateSupercell(self, ncell: int, radius: float) -> np.ndarray:
         return L.truncate_supercell(self.ndim, self.bravaisLattice, ncell, radius)
-
-
-class ResultTB:
-    """Eigen-pairs of the BSE (Result.hpp: eigval, eigvec columns = states)."""
-
-    def __init__(self, exciton: "ExcitonTB", eigval: np.ndarray, eigvec: Optional[np.ndarray]):
-        self.exciton = exciton
-        self.eigval = eigval
-        self.eigvec = eigvec
 
 
 class ExcitonTB:
