@@ -51,8 +51,9 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true", help="skip the differentiation workload")
     p.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     p.add_argument("--batch-count", type=int, default=64)
-    p.add_argument("--workload", default="config2", choices=["config2", "config1", "config3"],
-                   help="config2: the headline line (default); config1 / config3: one JSON line for that workload")
+    p.add_argument("--workload", default="config2", choices=["config2", "config1", "config3", "postproc"],
+                   help="config2: the headline line (default); config1 / config3 / postproc: one JSON line for "
+                        "that workload")
     p.add_argument("--adjoint-ncell", type=int, default=48)
     return p.parse_args()
 
@@ -645,6 +646,92 @@ def config3_run() -> dict:
             "max_abs_dE_eV_lowest16": float(np.abs(rm.eigval[:16] - rf.eigval[:16]).max())}
 
 
+def postproc_run(ncell: int, reps: int = 5, cpu: bool = True) -> dict:
+    """Post-processing of the headline system (N = 14400, lowest 8 states of the mixed solve) through the
+    ResultTB interface, each call from host coefficients to host results (median of reps after 2 warm-ups):
+    state observables (kinetic energy, k weights, peaks), real-space amplitudes of all 8 states with the hole
+    on atom 0 over the cells within |a1| * ncell (the range of the reference's w.f. test), the envelope
+    transform at the same cells, and the absorption spectrum (400 frequencies, Lorentzian).  The CPU figure
+    times the oracle's numpy restatement of realSpaceWavefunction on a bounded sample of (cell, atom) values
+    and extrapolates to the full table (one host thread)."""
+    import torch
+    from xatu_b200.exciton import ExcitonTB
+    from xatu_b200.synthetic import synthetic_hexagonal
+    nst = WORKLOAD["nstates"]
+    ex = ExcitonTB(synthetic_hexagonal(seed=1234), ncell, 2, 0, WORKLOAD["params"])
+    ex.brillouinZoneMesh(ncell)
+    ex.initializeHamiltonian()
+    ex.BShamiltonian("mixed")
+    res = ex.diagonalize("davidson", nst)
+    s = ex.system
+    cells = s.truncateSupercell(ncell, float(np.linalg.norm(s.bravaisLattice[0])) * ncell)
+    hole = 0
+    nho = int(s.orbitals[int(s.motif[hole, 3])])
+    P = nst * s.basisdim * nho
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    launches0 = ex.kernelLaunches()
+    t_obs = timed(lambda: res.observables())
+    t_rs = timed(lambda: res.realSpaceAmplitudes(res.eigvec, hole, np.zeros(3), cells))
+    t_env = timed(lambda: res.ftExcitonEnvelopes(res.eigvec, cells))
+    t_abs = timed(lambda: res.absorptionSpectrum(1.0, 6.0, 400, 0.08, "lorentzian"))
+    launches = ex.kernelLaunches() - launches0
+    # FP64 reference rate: cuBLAS DGEMM (torch.matmul on float64) at 8192^3, the denominator of the transform
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    dgemm_tflops = 5 * 2.0 * 8192 ** 3 / (time.perf_counter() - t0) / 1e12
+    del a, b
+    out = {"workload": f"postproc: {WORKLOAD['model']}, Nk={ncell}x{ncell}, N={ex.excitonbasisdim}, {nst} states "
+                       f"(mixed Davidson), {cells.shape[0]} cells within |a1|*{ncell}, hole on atom {hole}",
+           "unit": "ms per call (C ABI, host coefficients in, host results out)",
+           "observables_ms": t_obs * 1e3, "realspace_ms": t_rs * 1e3, "envelope_ms": t_env * 1e3,
+           "absorption_ms": t_abs * 1e3, "realspace_pairs": P,
+           "realspace_transform_fp64_flop": 8.0 * cells.shape[0] * s.nk * P,
+           "realspace_transform_tflops_incl_call": 8.0 * cells.shape[0] * s.nk * P / t_rs / 1e12,
+           "fp64_dgemm_tflops_measured": dgemm_tflops,
+           "gpu_launches": int(launches)}
+    if cpu:
+        from oracle.oracle import OracleExciton, OracleSystem
+        from oracle.postproc import real_space_wavefunction
+        si = synthetic_hexagonal(seed=1234).systemInfo
+        o = OracleExciton(OracleSystem(si.ndim, si.bravaisLattice, si.motif, si.norbitals, si.bravaisVectors,
+                                       si.hamiltonian, int(si.filling)), ncell, 2, 0, WORKLOAD["params"])
+        o.brillouin_zone_mesh(ncell)
+        o.initialize_hamiltonian()
+        x = res.eigvec[:, 0]
+        t0 = time.perf_counter()
+        done = 0
+        while time.perf_counter() - t0 < 8.0 and done < cells.shape[0] * s.natoms:
+            ci, atom = divmod(done, s.natoms)
+            real_space_wavefunction(o, x, atom, hole, cells[ci], np.zeros(3))
+            done += 1
+        t_sample = time.perf_counter() - t0
+        full = nst * cells.shape[0] * s.natoms
+        out["cpu_baseline"] = {"value": t_sample / done * full * 1e3, "unit": "ms (real-space table)",
+                               "cores": 1, "kind": "port",
+                               "sample": f"oracle numpy realSpaceWavefunction, {done} of {full} (state, cell, atom) "
+                                         f"values in {t_sample:.1f} s, scaled to the full table"}
+    ex.close()
+    return out
+
+
 def main():
     args = parse()
     # the engine library (and the toolkit's cuSOLVER / cuBLAS it links) before torch's bundled copies
@@ -652,7 +739,9 @@ def main():
     if os.path.exists(L.LIB_PATH):
         L.lib()
     if args.workload != "config2":
-        print(json.dumps(config1_run() if args.workload == "config1" else config3_run()), flush=True)
+        runs = {"config1": config1_run, "config3": config3_run,
+                "postproc": lambda: postproc_run(args.ncell, cpu=not args.no_cpu)}
+        print(json.dumps(runs[args.workload]()), flush=True)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -18,6 +18,7 @@
 //                       Gaussian delta of get_kubo_intens and the broadened exciton oscillator strengths.
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstring>
 
 #include "engine.h"
@@ -205,70 +206,101 @@ extern "C" __global__ void pp_weights_to_f_kernel(int nk, int ns, const double* 
   F[idx] = mk(kweight[(long long)s * nk + k], 0.0);
 }
 
-#define DFT_TC 64    // points per CTA (8 per warp)
 #define DFT_TK 16    // k points per shared-memory stage
 
-// part[z][pt][p] = sum_{k in split z} exp(i sign k.d_pt) F[k][p].  PT pairs per CTA on lanes; the 32 / PT lane
-// groups take interleaved k of each stage and are summed by a fixed butterfly at the end.
-template <int PT>
-__global__ void __launch_bounds__(256) pp_kdft_kernel(int nk, int P, const double* __restrict__ kpts,
-                                                      const cd* __restrict__ F, int npts,
-                                                      const double* __restrict__ pts, double sign, int kchunk,
-                                                      cd* __restrict__ part) {
-  __shared__ cd ph[DFT_TC][DFT_TK + 1];
-  __shared__ cd fs[DFT_TK][PT];
-  __shared__ double dp[DFT_TC][3];
-  __shared__ double kp[DFT_TK][3];
+// part[z][pt][p] = sum_{k in split z} exp(i sign k.d_pt) F[k][p].  A CTA covers 8*CPW points x PT*NPL pairs:
+// the phase tile (8*CPW points x 16 k) is evaluated once per stage in shared memory and shared by all pairs of
+// the CTA; lane l holds pairs l % PT + j*PT (j < NPL) for the CPW points of its warp, so each phase read feeds
+// NPL complex products and each F read feeds CPW.  With PT < 32 the 32 / PT lane groups take interleaved k of
+// each stage and are summed by a fixed butterfly at the end (deterministic for a given launch shape).
+template <int PT, int NPL, int CPW>
+constexpr size_t pp_kdft_smem() {
+  return sizeof(double2) * ((size_t)8 * CPW * (DFT_TK + 1) + (size_t)DFT_TK * PT * NPL) +
+         sizeof(double) * 3 * (8 * CPW + DFT_TK);
+}
+
+template <int PT, int NPL, int CPW>
+__global__ void __launch_bounds__(256, 2) pp_kdft_kernel(int nk, int P, const double* __restrict__ kpts,
+                                                         const cd* __restrict__ F, int npts,
+                                                         const double* __restrict__ pts, double sign, int kchunk,
+                                                         cd* __restrict__ part) {
+  constexpr int PW = PT * NPL;   // pairs per CTA
+  constexpr int TC = 8 * CPW;    // points per CTA
+  extern __shared__ __align__(16) unsigned char pp_smem[];
+  auto ph = reinterpret_cast<double2(*)[DFT_TK + 1]>(pp_smem);                                   // [TC][TK + 1]
+  auto fs = reinterpret_cast<double2(*)[PW]>(pp_smem + sizeof(double2) * TC * (DFT_TK + 1));        // [TK][PW]
+  auto dp = reinterpret_cast<double(*)[3]>(pp_smem + sizeof(double2) * (TC * (DFT_TK + 1) + DFT_TK * PW));
+  auto kp = dp + TC;                                                                             // [TK][3]
   constexpr int KS = 32 / PT;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int pl = lane % PT, ks = lane / PT;
-  const int pt0 = blockIdx.x * DFT_TC, p0 = blockIdx.y * PT;
+  const int pt0 = blockIdx.x * TC, p0 = blockIdx.y * PW;
   const int kbeg = blockIdx.z * kchunk, kend = min(nk, kbeg + kchunk);
-  for (int t = tid; t < DFT_TC * 3; t += blockDim.x) {
+  for (int t = tid; t < TC * 3; t += blockDim.x) {
     const int c = t / 3, d = t - c * 3;
     dp[c][d] = (pt0 + c < npts) ? pts[(long long)(pt0 + c) * 3 + d] : 0.0;
   }
-  cd acc[8];
+  double2 acc[CPW][NPL];
 #pragma unroll
-  for (int c = 0; c < 8; c++) acc[c] = mk(0, 0);
+  for (int c = 0; c < CPW; c++)
+#pragma unroll
+    for (int j = 0; j < NPL; j++) acc[c][j] = make_double2(0.0, 0.0);
   for (int k0 = kbeg; k0 < kend; k0 += DFT_TK) {
     __syncthreads();   // the previous stage is consumed (and dp is visible on the first pass)
     if (tid < DFT_TK * 3) {
       const int kk = tid / 3, d = tid - kk * 3;
       kp[kk][d] = (k0 + kk < kend) ? kpts[(long long)(k0 + kk) * 3 + d] : 0.0;
     }
-    for (int t = tid; t < DFT_TK * PT; t += blockDim.x) {
-      const int kk = t / PT, q = t - kk * PT;
-      fs[kk][q] = (k0 + kk < kend && p0 + q < P) ? F[(long long)(k0 + kk) * P + p0 + q] : mk(0, 0);
+    for (int t = tid; t < DFT_TK * PW; t += blockDim.x) {
+      const int kk = t / PW, q = t - kk * PW;
+      cd f = mk(0, 0);
+      if (k0 + kk < kend && p0 + q < P) f = F[(long long)(k0 + kk) * P + p0 + q];
+      fs[kk][q] = make_double2(f.x, f.y);
     }
     __syncthreads();
-    for (int t = tid; t < DFT_TC * DFT_TK; t += blockDim.x) {
+    for (int t = tid; t < TC * DFT_TK; t += blockDim.x) {
       const int c = t / DFT_TK, kk = t - c * DFT_TK;
       const double x = kp[kk][0] * dp[c][0] + kp[kk][1] * dp[c][1] + kp[kk][2] * dp[c][2];
       double sn, cs;
       sincos(x, &sn, &cs);
-      ph[c][kk] = mk(cs, sign * sn);
+      ph[c][kk] = make_double2(cs, sign * sn);
     }
     __syncthreads();
     for (int kk = ks; kk < DFT_TK; kk += KS) {
-      const cd f = fs[kk][pl];
+      double2 f[NPL];
 #pragma unroll
-      for (int c = 0; c < 8; c++) acc[c] = acc[c] + ph[warp * 8 + c][kk] * f;
+      for (int j = 0; j < NPL; j++) f[j] = fs[kk][pl + j * PT];
+#pragma unroll
+      for (int c = 0; c < CPW; c++) {
+        const double2 e = ph[warp * CPW + c][kk];
+#pragma unroll
+        for (int j = 0; j < NPL; j++) {
+          acc[c][j].x = fma(e.x, f[j].x, fma(-e.y, f[j].y, acc[c][j].x));
+          acc[c][j].y = fma(e.x, f[j].y, fma(e.y, f[j].x, acc[c][j].y));
+        }
+      }
     }
   }
 #pragma unroll
   for (int o = PT; o < 32; o <<= 1) {
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, o);
-      acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, o);
-    }
-  }
-  if (ks == 0 && p0 + pl < P) {
+    for (int c = 0; c < CPW; c++)
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int pt = pt0 + warp * 8 + c;
-      if (pt < npts) part[((long long)blockIdx.z * npts + pt) * P + p0 + pl] = acc[c];
+      for (int j = 0; j < NPL; j++) {
+        acc[c][j].x += __shfl_xor_sync(0xffffffffu, acc[c][j].x, o);
+        acc[c][j].y += __shfl_xor_sync(0xffffffffu, acc[c][j].y, o);
+      }
+  }
+  if (ks == 0) {
+#pragma unroll
+    for (int j = 0; j < NPL; j++) {
+      const int p = p0 + pl + j * PT;
+      if (p >= P) continue;
+#pragma unroll
+      for (int c = 0; c < CPW; c++) {
+        const int pt = pt0 + warp * CPW + c;
+        if (pt < npts) part[((long long)blockIdx.z * npts + pt) * P + p] = mk(acc[c][j].x, acc[c][j].y);
+      }
     }
   }
 }
@@ -502,26 +534,68 @@ extern "C" xatu_status xatu_state_observables(xatu_ctx* ctx, int nstates, const 
   return XATU_OK;
 }
 
-// Launch shape of pp_kdft_kernel: pairs per CTA (PT), k splits and the k range of a split.
+// Launch shape of pp_kdft_kernel: lanes per pair tile (PT), pairs per lane (NPL; 4 pairs with 4 points per
+// warp, otherwise 8 points per warp), k splits and the k range of a split.  The split count fills the GPU and,
+// among up to 8 splits, keeps the last wave of CTAs fullest.
 struct KdftPlan {
-  int PT, nsplit, kchunk;
+  int PT, NPL, CPW, nsplit, kchunk;
   dim3 grid;
 };
+
+#define PP_KDFT_VARIANTS(X) \
+  X(1, 1, 8) X(2, 1, 8) X(4, 1, 8) X(8, 1, 8) X(16, 1, 8) X(32, 1, 8) X(32, 2, 8) X(32, 4, 4)
+
+static const void* pp_kdft_fn(int PT, int NPL, int CPW) {
+#define PP_FN(A, B, C) \
+  if (PT == A && NPL == B && CPW == C) return (const void*)pp_kdft_kernel<A, B, C>;
+  PP_KDFT_VARIANTS(PP_FN)
+#undef PP_FN
+  return nullptr;
+}
+
+static size_t pp_kdft_smem_of(int PT, int NPL, int CPW) {
+#define PP_SM(A, B, C) \
+  if (PT == A && NPL == B && CPW == C) return pp_kdft_smem<A, B, C>();
+  PP_KDFT_VARIANTS(PP_SM)
+#undef PP_SM
+  return 0;
+}
 
 static KdftPlan pp_kdft_plan(const xatu_ctx* ctx, int P, int npts) {
   KdftPlan pl;
   const int nk = ctx->nk;
   pl.PT = 1;
   while (pl.PT < 32 && pl.PT < P) pl.PT <<= 1;
-  const long long tiles = (long long)((npts + DFT_TC - 1) / DFT_TC) * ((P + pl.PT - 1) / pl.PT);
+  pl.NPL = (P >= 128) ? 4 : (P > 32) ? 2 : 1;
+  pl.CPW = (pl.NPL == 4) ? 4 : 8;
+  const int PW = pl.PT * pl.NPL, TC = 8 * pl.CPW;
+  const long long tiles = (long long)((npts + TC - 1) / TC) * ((P + PW - 1) / PW);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pp_kdft_fn(pl.PT, pl.NPL, pl.CPW), 256,
+                                                    pp_kdft_smem_of(pl.PT, pl.NPL, pl.CPW)) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long slots = (long long)per_sm * ctx->num_sms;
   const int max_split = std::max(1, (nk + 4 * DFT_TK - 1) / (4 * DFT_TK));
-  const long long want = (2LL * ctx->num_sms + tiles - 1) / tiles;
-  int nsplit = (int)std::max(1LL, std::min<long long>(want, max_split));
+  int nsplit = 1;
+  if (tiles < slots) {
+    nsplit = (int)std::min<long long>((slots + tiles - 1) / tiles, max_split);
+  } else {
+    double best = -1.0;
+    for (int z = 1; z <= std::min(8, max_split); z++) {
+      const double waves = (double)(tiles * z) / (double)slots;
+      const double eff = waves / std::ceil(waves);
+      if (eff > best + 0.02) {
+        best = eff;
+        nsplit = z;
+      }
+    }
+  }
   int kchunk = (nk + nsplit - 1) / nsplit;
   kchunk = (kchunk + DFT_TK - 1) / DFT_TK * DFT_TK;
   pl.nsplit = (nk + kchunk - 1) / kchunk;
   pl.kchunk = kchunk;
-  pl.grid = dim3((unsigned)((npts + DFT_TC - 1) / DFT_TC), (unsigned)((P + pl.PT - 1) / pl.PT), (unsigned)pl.nsplit);
+  pl.grid = dim3((unsigned)((npts + TC - 1) / TC), (unsigned)((P + PW - 1) / PW), (unsigned)pl.nsplit);
   return pl;
 }
 
@@ -535,14 +609,13 @@ static xatu_status pp_kdft(xatu_ctx* ctx, const KdftPlan& pl, const cd* F, int P
   cd* part = ctx->d_pp_P.as<cd>();
   const dim3 g = pl.grid;
   const int kc = pl.kchunk;
-  switch (pl.PT) {
-    case 1: pp_kdft_kernel<1><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-    case 2: pp_kdft_kernel<2><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-    case 4: pp_kdft_kernel<4><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-    case 8: pp_kdft_kernel<8><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-    case 16: pp_kdft_kernel<16><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-    default: pp_kdft_kernel<32><<<g, 256, 0, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part); break;
-  }
+  const size_t sm = pp_kdft_smem_of(pl.PT, pl.NPL, pl.CPW);
+  XATU_CK(xatu_raise_smem_limit(pp_kdft_fn(pl.PT, pl.NPL, pl.CPW), sm));
+#define PP_LAUNCH(A, B, C)                                                                                 \
+  if (pl.PT == A && pl.NPL == B && pl.CPW == C)                                                            \
+    pp_kdft_kernel<A, B, C><<<g, 256, sm, ctx->stream>>>(nk, P, kp, F, npts, dpts, sign, kc, part);
+  PP_KDFT_VARIANTS(PP_LAUNCH)
+#undef PP_LAUNCH
   ctx->launches++;
   XATU_CK_LAUNCH("pp_kdft_kernel");
   return XATU_OK;
