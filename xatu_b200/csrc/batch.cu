@@ -15,12 +15,14 @@
 //     reads the number of systems still active.  Converged systems skip their
 //     work, the tcgen05 K.X product included.
 //
-// Davidson step of one system (basis V, W = H V kept in Ritz form, block P of
-// at most BD_MAXB new directions):
+// Davidson step of one system (basis V, W = H V, projected matrix T = V^H W
+// grown by the new columns only; block P of at most BD_MAXB new directions):
 //   W_P = H P (split-BF16 K on tcgen05 + FP64 band diagonal);  append P, W_P;
-//   T = V^H W (new columns);  Jacobi eigensolve of T;  V <- V Y, W <- W Y;
-//   r_j = W_j - theta_j V_j,  P_j = r_j / (theta_j - H_jj)  (j < block);
-//   converged when max_{j < nstates} |r_j| < tol;  restart = truncation to the block;
+//   T[:, new] = V^H W_P;  lowest block of Ritz pairs of T (eigh_small.cuh);
+//   U = V Y, WU = W Y (block columns only);
+//   r_j = WU_j - theta_j U_j,  P_j = r_j / (theta_j - H_jj)  (j < block);
+//   converged when max_{j < nstates} |r_j| < tol;
+//   restart (basis full): V <- U, W <- WU, T <- diag(theta);
 //   P orthonormalised (eigen-decomposition of its Gram matrix), projected out of
 //   V twice (classical Gram-Schmidt), orthonormalised again; directions whose
 //   norm falls below the threshold are dropped.
@@ -32,6 +34,7 @@
 #include <string>
 #include <vector>
 
+#include "eigh_small.cuh"
 #include "engine.h"
 #include "jacobi.cuh"
 #include "kernels.h"
@@ -42,8 +45,7 @@
 #define BD_MAXB 16            // largest Davidson block
 #define BD_MMAX 64            // largest basis
 #define BD_EIGH_THREADS 256
-#define BD_RR_THREADS 512
-#define BD_ROT_ROWS 32
+#define BD_RR_THREADS HEEV_THREADS
 
 struct BDav {
   long long N, ldk, ldb;
@@ -54,9 +56,11 @@ struct BDav {
   cd* V;                    // N x mmax, column-major
   cd* W;
   cd* P;                    // N x BD_MAXB
-  cd* WP;
-  cd* T;                    // mmax x mmax (ld BD_MMAX)
-  cd* Y;
+  cd* U;                    // N x BD_MAXB: Ritz vectors of the block
+  cd* WU;                   // N x BD_MAXB: W Y
+  cd* T;                    // mmax x mmax (ld BD_MMAX), both triangles
+  cd* Y;                    // mmax x BD_MAXB (ld BD_MMAX): Ritz coefficients
+  cd* R;                    // mmax x mmax: reflector scratch of the Rayleigh-Ritz eigensolver
   cd* C1;                   // BD_MMAX x BD_MAXB (ld BD_MMAX)
   cd* C2;
   cd* G1;                   // BD_MAXB x BD_MAXB (ld BD_MAXB)
@@ -67,7 +71,7 @@ struct BDav {
   float* Yf;                // N x 2 bp (tcgen05 output)
   __nv_bfloat16* Bhi;       // 2 bp x ldb
   __nv_bfloat16* Blo;
-  int m, k, active, iters, stalled, kmask;
+  int m, k, active, iters, stalled, kmask, restart;
 };
 
 struct BDGlobal {
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(BD_ROWS) bd_residual_kernel(BDGlobal g, BDav* 
     double n2 = 0.0;
     if (i < d.N) {
       const double th = d.theta[j];
-      const cd u = d.V[(long long)j * d.N + i], wv = d.W[(long long)j * d.N + i];
+      const cd u = d.U[(long long)j * d.N + i], wv = d.WU[(long long)j * d.N + i];
       const cd r = mk(wv.x - th * u.x, wv.y - th * u.y);
       n2 = nrm2(r);
       double den = th - d.diagH[i];
@@ -226,58 +230,52 @@ __global__ void __launch_bounds__(BD_ROWS) bd_cgs_update_kernel(BDGlobal g, BDav
     if (s < g.bsz) d.P[(long long)s * d.N + i] = d.P[(long long)s * d.N + i] - acc[s];
 }
 
-// V[:, 0:m] <- V[:, 0:m] Y and W likewise, BD_ROT_ROWS rows per block staged in shared memory; each
-// thread accumulates a 2-row x 4-column register tile (6 shared loads per 8 complex multiply-adds).
-__global__ void __launch_bounds__(256) bd_rotate_kernel(BDGlobal g, BDav* D, const int* __restrict__ off) {
+// U = V[:, 0:m] Y, WU = W[:, 0:m] Y for the bsz block columns: one thread per row, Y in shared memory
+// (broadcast reads), V and W read once per row in coalesced column order.
+__global__ void __launch_bounds__(BD_ROWS) bd_ritz_kernel(BDGlobal g, BDav* D, const int* __restrict__ off) {
   const int mem = bd_member(off, g.nmem, blockIdx.x);
   const BDav& d = D[mem];
   if (!d.active) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  constexpr int LD = BD_MMAX + 1;
+  __shared__ cd sY[BD_MMAX * BD_MAXB];
   const int m = d.m;
-  cd* sY = reinterpret_cast<cd*>(smem_raw);        // m x m, row j at j * LD
-  cd* sA = sY + BD_MMAX * LD;                       // BD_ROT_ROWS x m, row r at r * LD
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+  for (int t = threadIdx.x; t < m * g.bsz; t += blockDim.x) {
     const int r = t % m, c = t / m;
-    sY[r * LD + c] = d.Y[r + c * BD_MMAX];
+    sY[r * BD_MAXB + c] = d.Y[r + c * BD_MMAX];
   }
-  const long long row0 = (long long)(blockIdx.x - off[mem]) * BD_ROT_ROWS;
-  const int rows = (int)min((long long)BD_ROT_ROWS, d.N - row0);
-  const int rg = threadIdx.x >> 4, cg = threadIdx.x & 15;   // rows 2rg, 2rg+1; columns 4cg .. 4cg+3
-  for (int mat = 0; mat < 2; mat++) {
-    cd* A = mat == 0 ? d.V : d.W;
-    __syncthreads();
-    for (int t = threadIdx.x; t < BD_ROT_ROWS * m; t += blockDim.x) {
-      const int r = t % BD_ROT_ROWS, c = t / BD_ROT_ROWS;
-      sA[r * LD + c] = (r < rows) ? A[(long long)c * d.N + row0 + r] : mk(0, 0);
-    }
-    __syncthreads();
-    if (4 * cg < m) {
-      cd acc[2][4];
+  __syncthreads();
+  const long long i = (long long)(blockIdx.x - off[mem]) * BD_ROWS + threadIdx.x;
+  if (i >= d.N) return;
+  cd au[BD_MAXB], aw[BD_MAXB];
 #pragma unroll
-      for (int i = 0; i < 2; i++)
+  for (int s = 0; s < BD_MAXB; s++) au[s] = aw[s] = mk(0, 0);
+  for (int j = 0; j < m; j++) {
+    const cd v = d.V[(long long)j * d.N + i], w = d.W[(long long)j * d.N + i];
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[i][q] = mk(0, 0);
-      for (int j = 0; j < m; j++) {
-        const cd a0 = sA[(2 * rg) * LD + j], a1 = sA[(2 * rg + 1) * LD + j];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const cd y = sY[j * LD + 4 * cg + q];
-          acc[0][q] = acc[0][q] + a0 * y;
-          acc[1][q] = acc[1][q] + a1 * y;
-        }
+    for (int s = 0; s < BD_MAXB; s++)
+      if (s < g.bsz) {
+        const cd y = sY[j * BD_MAXB + s];
+        au[s] = au[s] + v * y;
+        aw[s] = aw[s] + w * y;
       }
+  }
 #pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const int r = 2 * rg + i;
-        if (r >= rows) continue;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const int c = 4 * cg + q;
-          if (c < m) A[(long long)c * d.N + row0 + r] = acc[i][q];
-        }
-      }
+  for (int s = 0; s < BD_MAXB; s++)
+    if (s < g.bsz) {
+      d.U[(long long)s * d.N + i] = au[s];
+      d.WU[(long long)s * d.N + i] = aw[s];
     }
+}
+
+// Thick restart of the members that decided one: V[:, 0:bsz] = U, W[:, 0:bsz] = WU.
+__global__ void __launch_bounds__(BD_ROWS) bd_restart_kernel(BDGlobal g, BDav* D, const int* __restrict__ off) {
+  const int mem = bd_member(off, g.nmem, blockIdx.x);
+  const BDav& d = D[mem];
+  if (!d.active || !d.restart) return;
+  const long long i = (long long)(blockIdx.x - off[mem]) * BD_ROWS + threadIdx.x;
+  if (i >= d.N) return;
+  for (int s = 0; s < g.bsz; s++) {
+    d.V[(long long)s * d.N + i] = d.U[(long long)s * d.N + i];
+    d.W[(long long)s * d.N + i] = d.WU[(long long)s * d.N + i];
   }
 }
 
@@ -412,50 +410,35 @@ __global__ void bd_prep_kernel(BDGlobal g, BDav* D) {
   }
 }
 
-// Hermitise the new block of T, Jacobi eigensolve, Ritz values and coefficients; m <- m + k.
+// Make the new columns of T exactly Hermitian (new x new block: the average of both triangles; the rows of
+// the new columns in the old columns by conjugation), then the lowest bsz Ritz pairs of T; m <- m + k.
 __global__ void __launch_bounds__(BD_RR_THREADS) bd_rr_kernel(BDGlobal g, BDav* D, int* status) {
   BDav& d = D[blockIdx.x];
   if (!d.active) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int m0 = d.m, m = d.m + d.k;
-  const int lda = m + 1;
-  cd* A = reinterpret_cast<cd*>(smem_raw);
-  cd* Vs = A + (size_t)m * lda;
-  JacobiRot* rot = reinterpret_cast<JacobiRot*>(Vs + (size_t)m * m);
-  double* scratch = reinterpret_cast<double*>(rot + (m / 2 + 2));
-  int* perm = reinterpret_cast<int*>(scratch + 64);
   cd* T = d.T;
-  // old block: diag(theta); new columns: the projection (all rows); new rows: by conjugation;
-  // new x new block: the average of both triangles (exactly Hermitian)
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int r = t % m, c = t / m;
-    cd v;
+  const int nn = d.k;
+  for (int t = threadIdx.x; t < m * nn; t += blockDim.x) {
+    const int r = t % m, c = m0 + t / m;
     if (r < m0) {
-      v = T[r + (long long)c * BD_MMAX];
-    } else if (c < m0) {
-      v = conj(T[c + (long long)r * BD_MMAX]);
-    } else {
+      T[c + (long long)r * BD_MMAX] = conj(T[r + (long long)c * BD_MMAX]);
+    } else if (r >= c) {
       const cd a = T[r + (long long)c * BD_MMAX], bb = T[c + (long long)r * BD_MMAX];
-      v = (r == c) ? mk(a.x, 0.0) : mk(0.5 * (a.x + bb.x), 0.5 * (a.y - bb.y));
+      const cd v = (r == c) ? mk(a.x, 0.0) : mk(0.5 * (a.x + bb.x), 0.5 * (a.y - bb.y));
+      T[r + (long long)c * BD_MMAX] = v;
+      T[c + (long long)r * BD_MMAX] = conj(v);
     }
-    A[r * lda + c] = v;
   }
   __syncthreads();
-  BlockGroup grp;
-  const int sweeps = jacobi_eigh(grp, A, lda, Vs, m, m, rot, scratch, 60, 1e-14);
-  if (sweeps > 60 && threadIdx.x == 0) atomicOr(status, XATU_DEVERR_NOCONV);
-  jacobi_sort(grp, A, lda, m, perm);
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int c = t / m, r = t - c * m;
-    d.Y[r + (long long)c * BD_MMAX] = Vs[r * m + perm[c]];
-  }
-  for (int c = threadIdx.x; c < m; c += blockDim.x) d.theta[c] = A[perm[c] * lda + perm[c]].x;
+  const int nr = min(g.bsz, m);
+  heev_lowest(T, BD_MMAX, m, nr, d.theta, d.Y, BD_MMAX, d.R, smem_raw, status);
   for (int c = threadIdx.x; c < BD_MAXB; c += blockDim.x) d.norms[c] = 0.0;
   __syncthreads();
   if (threadIdx.x == 0) d.m = m;
 }
 
-// Convergence, restart, next targets; T <- diag(theta); zero the reduction targets.
+// Convergence, restart decision (T <- diag(theta) on restart), next targets; zero the reduction targets.
 __global__ void bd_control_kernel(BDGlobal g, BDav* D) {
   BDav& d = D[blockIdx.x];
   if (!d.active) return;
@@ -477,15 +460,18 @@ __global__ void bd_control_kernel(BDGlobal g, BDav* D) {
       d.active = 0;
       d.stalled = 1;
     }
-    s_restart = (d.m + g.bsz > g.mmax) ? 1 : 0;
-    if (d.active && s_restart) d.m = g.bsz;
+    s_restart = (d.active && d.m + g.bsz > g.mmax) ? 1 : 0;
+    d.restart = s_restart;
+    if (s_restart) d.m = g.bsz;
   }
   __syncthreads();
   if (!d.active) return;
-  const int m = d.m;
-  for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-    const int r = t % m, c = t / m;
-    d.T[r + (long long)c * BD_MMAX] = mk(r == c ? d.theta[r] : 0.0, 0.0);
+  if (s_restart) {
+    const int m = d.m;
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+      const int r = t % m, c = t / m;
+      d.T[r + (long long)c * BD_MMAX] = mk(r == c ? d.theta[r] : 0.0, 0.0);
+    }
   }
   for (int t = threadIdx.x; t < BD_MMAX * BD_MAXB; t += blockDim.x) {
     d.C1[t] = mk(0, 0);
@@ -585,8 +571,8 @@ struct xatu_batch {
   BDGlobal g{};
   BDGlobal chosen{};
   std::vector<BDav> hdesc;
-  DBuf d_desc, d_row_off, d_red_off, d_rot_off, d_count, d_status, d_arena;
-  int nrow = 0, nred = 0, nrot = 0;
+  DBuf d_desc, d_row_off, d_red_off, d_count, d_status, d_arena;
+  int nrow = 0, nred = 0;
   int* h_count = nullptr;        // pinned
   cudaGraphExec_t build_exec = nullptr, iter_exec = nullptr;
   cudaEvent_t ev[4] = {};
@@ -727,12 +713,7 @@ static xatu_status enqueue_build(xatu_batch* b, bool with_assembly, bool with_in
   return XATU_OK;
 }
 
-static size_t rr_smem() {
-  const int m = BD_MMAX;
-  return (size_t)m * (m + 1) * sizeof(cd) + (size_t)m * m * sizeof(cd) + (m / 2 + 2) * sizeof(JacobiRot) +
-         64 * sizeof(double) + (m + 1) * sizeof(int);
-}
-static size_t rot_smem() { return (size_t)(BD_MMAX + BD_ROT_ROWS) * (BD_MMAX + 1) * sizeof(cd); }
+static size_t rr_smem() { return heev_smem_bytes(BD_MMAX, BD_MAXB); }
 
 // One Davidson step for every active member.
 static xatu_status enqueue_iteration(xatu_batch* b) {
@@ -753,9 +734,10 @@ static xatu_status enqueue_iteration(xatu_batch* b) {
   bd_prep_kernel<<<g.nmem, 256, 0, b->stream>>>(g, D);
   bd_gemm_h_kernel<<<b->nred, 256, 0, b->stream>>>(g, D, rd, 0);
   bd_rr_kernel<<<g.nmem, BD_RR_THREADS, rr_smem(), b->stream>>>(g, D, status);
-  bd_rotate_kernel<<<b->nrot, 256, rot_smem(), b->stream>>>(g, D, b->d_rot_off.as<int>());
+  bd_ritz_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_residual_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_control_kernel<<<g.nmem, 256, 0, b->stream>>>(g, D);
+  bd_restart_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_gemm_h_kernel<<<b->nred, 256, 0, b->stream>>>(g, D, rd, 3);
   bd_orth_kernel<<<g.nmem, BD_EIGH_THREADS, 0, b->stream>>>(g, D, 0, status);
   bd_apply_s_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
@@ -883,8 +865,8 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     const long long N = b->members[i]->N;
     const long long ldb = (2 * N + 7) / 8 * 8;
     offs[i] = total;
-    total += al(N * sizeof(double)) + 2 * al((size_t)N * mmax * sizeof(cd)) + 2 * al((size_t)N * BD_MAXB * sizeof(cd)) +
-             2 * al((size_t)BD_MMAX * BD_MMAX * sizeof(cd)) + 2 * al((size_t)BD_MMAX * BD_MAXB * sizeof(cd)) +
+    total += al(N * sizeof(double)) + 2 * al((size_t)N * mmax * sizeof(cd)) + 3 * al((size_t)N * BD_MAXB * sizeof(cd)) +
+             3 * al((size_t)BD_MMAX * BD_MMAX * sizeof(cd)) + 2 * al((size_t)BD_MMAX * BD_MAXB * sizeof(cd)) +
              3 * al((size_t)BD_MAXB * BD_MAXB * sizeof(cd)) + al(BD_MMAX * sizeof(double)) +
              al(BD_MAXB * sizeof(double)) + al((size_t)N * 2 * b->g.bp * sizeof(float)) +
              2 * al((size_t)2 * b->g.bp * ldb * sizeof(__nv_bfloat16));
@@ -912,9 +894,11 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     d.V = reinterpret_cast<cd*>(take((size_t)N * mmax * sizeof(cd)));
     d.W = reinterpret_cast<cd*>(take((size_t)N * mmax * sizeof(cd)));
     d.P = reinterpret_cast<cd*>(take((size_t)N * BD_MAXB * sizeof(cd)));
-    d.WP = reinterpret_cast<cd*>(take((size_t)N * BD_MAXB * sizeof(cd)));
+    d.U = reinterpret_cast<cd*>(take((size_t)N * BD_MAXB * sizeof(cd)));
+    d.WU = reinterpret_cast<cd*>(take((size_t)N * BD_MAXB * sizeof(cd)));
     d.T = reinterpret_cast<cd*>(take((size_t)BD_MMAX * BD_MMAX * sizeof(cd)));
     d.Y = reinterpret_cast<cd*>(take((size_t)BD_MMAX * BD_MMAX * sizeof(cd)));
+    d.R = reinterpret_cast<cd*>(take((size_t)BD_MMAX * BD_MMAX * sizeof(cd)));
     d.C1 = reinterpret_cast<cd*>(take((size_t)BD_MMAX * BD_MAXB * sizeof(cd)));
     d.C2 = reinterpret_cast<cd*>(take((size_t)BD_MMAX * BD_MAXB * sizeof(cd)));
     d.G1 = reinterpret_cast<cd*>(take((size_t)BD_MAXB * BD_MAXB * sizeof(cd)));
@@ -929,29 +913,24 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   BCK(b->d_desc.ensure(nmem * sizeof(BDav)));
   BCK(cudaMemcpyAsync(b->d_desc.p, b->hdesc.data(), nmem * sizeof(BDav), cudaMemcpyHostToDevice, b->stream));
   // chunk offsets
-  std::vector<int> ro(nmem + 1), rd(nmem + 1), rt(nmem + 1);
-  ro[0] = rd[0] = rt[0] = 0;
+  std::vector<int> ro(nmem + 1), rd(nmem + 1);
+  ro[0] = rd[0] = 0;
   for (int i = 0; i < nmem; i++) {
     const long long N = b->members[i]->N;
     ro[i + 1] = ro[i] + (int)((N + BD_ROWS - 1) / BD_ROWS);
     rd[i + 1] = rd[i] + (int)((N + BD_RED_ROWS - 1) / BD_RED_ROWS);
-    rt[i + 1] = rt[i] + (int)((N + BD_ROT_ROWS - 1) / BD_ROT_ROWS);
   }
   b->nrow = ro[nmem];
   b->nred = rd[nmem];
-  b->nrot = rt[nmem];
   BCK(b->d_row_off.ensure((nmem + 1) * sizeof(int)));
   BCK(b->d_red_off.ensure((nmem + 1) * sizeof(int)));
-  BCK(b->d_rot_off.ensure((nmem + 1) * sizeof(int)));
   BCK(cudaMemcpyAsync(b->d_row_off.p, ro.data(), ro.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaMemcpyAsync(b->d_red_off.p, rd.data(), rd.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
-  BCK(cudaMemcpyAsync(b->d_rot_off.p, rt.data(), rt.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   BCK(b->d_count.ensure(sizeof(int)));
   BCK(b->d_status.ensure(sizeof(int)));
   BCK(cudaMemsetAsync(b->d_status.p, 0, sizeof(int), b->stream));
   if (!b->h_count) BCK(cudaMallocHost(&b->h_count, sizeof(int)));
   BCK(xatu_raise_smem_limit((const void*)bd_rr_kernel, rr_smem()));
-  BCK(xatu_raise_smem_limit((const void*)bd_rotate_kernel, rot_smem()));
   BCK(cudaStreamSynchronize(b->stream));
   // graphs of every block candidate, each timed on a full solve; the fastest is kept
   std::string dav = "";
@@ -1025,7 +1004,7 @@ xatu_status xatu_batch_destroy(xatu_batch* b) {
     c.d_work.release();
     c.d_counter.release();
   }
-  for (DBuf* d : {&b->d_desc, &b->d_row_off, &b->d_red_off, &b->d_rot_off, &b->d_count, &b->d_status, &b->d_arena})
+  for (DBuf* d : {&b->d_desc, &b->d_row_off, &b->d_red_off, &b->d_count, &b->d_status, &b->d_arena})
     d->release();
   if (b->h_count) cudaFreeHost(b->h_count);
   for (xatu_ctx* c : b->members) xatu_ctx_destroy(c);
@@ -1102,7 +1081,7 @@ xatu_status xatu_batch_result(xatu_batch* b, int index, double* eigval, double* 
   if (!b->prepared) return bfail(b, XATU_ERR_STATE, "run the batch first");
   const BDav& d = b->hdesc[index];
   if (eigval) BCK(cudaMemcpy(eigval, d.theta, b->nstates * sizeof(double), cudaMemcpyDeviceToHost));
-  if (eigvec) BCK(cudaMemcpy(eigvec, d.V, (size_t)d.N * b->nstates * sizeof(cd), cudaMemcpyDeviceToHost));
+  if (eigvec) BCK(cudaMemcpy(eigvec, d.U, (size_t)d.N * b->nstates * sizeof(cd), cudaMemcpyDeviceToHost));
   return XATU_OK;
 }
 
