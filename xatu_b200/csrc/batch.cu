@@ -41,9 +41,10 @@
 
 #define BD_ROWS 64            // rows per chunk of the row kernels (one thread per row)
 #define BD_RED_ROWS 512       // rows per chunk of the reduction kernels
-#define BD_SUB 32             // rows staged per pass of a reduction
+#define BD_SUB 16             // rows staged per pass of a reduction
 #define BD_MAXB 16            // largest Davidson block
-#define BD_MMAX 64            // largest basis
+#define BD_BASIS_BLOCKS 6     // basis limit in blocks (restart beyond it)
+#define BD_MMAX (BD_BASIS_BLOCKS * BD_MAXB)   // largest basis
 #define BD_EIGH_THREADS 256
 #define BD_RR_THREADS HEEV_THREADS
 
@@ -809,13 +810,14 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   if ((b0 + 7) / 8 * 8 != b0 && (b0 + 7) / 8 * 8 <= BD_MAXB) blocks.push_back((b0 + 7) / 8 * 8);
   b->bsz = blocks.back();
   const int mmax = BD_MMAX;
+  auto basis_of = [](int bs) { return std::min(BD_MMAX, BD_BASIS_BLOCKS * bs); };
   // per-member buffers
   for (int i = 0; i < nmem; i++) {
     xatu_ctx* ctx = b->members[i];
     const long long N = ctx->N;
-    if (N < std::min(BD_MMAX, 4 * b0))
+    if (N < basis_of(b0))
       return bfail(b, XATU_ERR_UNSUPPORTED, "system " + std::to_string(i) + " is smaller than the basis");
-    if (N < mmax) blocks.resize(1);   // the larger block's basis would not fit this system
+    if (N < basis_of(blocks.back())) blocks.resize(1);   // the larger block's basis would not fit this system
     if (!xatu_assembly_batch_supported(ctx->nv, ctx->nc, ctx->natoms))
       return bfail(b, XATU_ERR_UNSUPPORTED, "system " + std::to_string(i) +
                                                 ": batched assembly supports 1-3 valence/conduction bands, 2-3 atoms");
@@ -940,7 +942,7 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     b->bsz = bs;
     b->g.bsz = bs;
     b->g.bp = (bs + 7) / 8 * 8;
-    b->g.mmax = std::min(BD_MMAX, 4 * bs);
+    b->g.mmax = basis_of(bs);
     cudaGraphExec_t be = nullptr, ie = nullptr;
     BTRY(capture(b, true, &be));
     BTRY(capture(b, false, &ie));
