@@ -139,25 +139,37 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         }
     }
   }
-  // coefficients: the k rows [band][orbital] are contiguous in global memory (valence part from the k
-  // stack, conduction part from the k+Q stack, same layout), so consecutive threads read consecutive
-  // elements of one k point; stored transposed, [side][band][orbital][kq] with padded rows
+  // coefficients: the TK k rows [band][orbital] of a side are one contiguous block in global memory
+  // (valence part from the k stack, conduction part from the k+Q stack, same layout), so consecutive
+  // threads read consecutive elements; each thread issues its loads in batches of 8 before storing them,
+  // transposed, to [side][band][orbital][kq] with padded rows
   {
     const int nbo = NB * norb;
+    const int per_side = TK * nbo;
+    const int total = 2 * per_side;
+    constexpr int BATCH = 8;
+    for (int t0 = tid; t0 < total; t0 += BATCH * blockDim.x) {
+      cd cv[BATCH];
 #pragma unroll
-    for (int side = 0; side < 2; side++) {
-      const int kbase = (side == 0 ? kb : kb2) * TK;
-      E* dst = sC + side * side_sz;
-      for (int kq = 0; kq < TK; kq++) {
-        const int k = kbase + kq;
-        if (k < p.nk) {
-          const int64_t row = (int64_t)k * p.nb * norb;
-          for (int e = tid; e < nbo; e += blockDim.x) {
-            const cd c = (e < NV * norb ? in.eigvec : in.eigvecQ)[row + e];
-            dst[e * TKP + kq] = E{(T)c.x, (T)c.y};
-          }
-        } else {
-          for (int e = tid; e < nbo; e += blockDim.x) dst[e * TKP + kq] = E{T(0), T(0)};
+      for (int q = 0; q < BATCH; q++) {
+        const int t = t0 + q * blockDim.x;
+        cv[q] = mk(0, 0);
+        if (t < total) {
+          const int side = t >= per_side ? 1 : 0;
+          const int r = t - side * per_side;
+          const int kq = r / nbo, e = r - kq * nbo;
+          const int k = (side ? kb2 : kb) * TK + kq;
+          if (k < p.nk) cv[q] = (e < NV * norb ? in.eigvec : in.eigvecQ)[(int64_t)k * p.nb * norb + e];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < BATCH; q++) {
+        const int t = t0 + q * blockDim.x;
+        if (t < total) {
+          const int side = t >= per_side ? 1 : 0;
+          const int r = t - side * per_side;
+          const int kq = r / nbo, e = r - kq * nbo;
+          sC[side * side_sz + e * TKP + kq] = E{(T)cv[q].x, (T)cv[q].y};
         }
       }
     }
