@@ -504,14 +504,35 @@ extern "C" cudaError_t xatu_launch_band_select(const BandParams& bp, const doubl
                                                cudaStream_t s) {
   const int nbs = bp.nb <= 4 ? 4 : (bp.nb <= 8 ? 8 : 16);
   const BsLayout Ly = bs_layout(bp.norb, bp.nR, nbs);
-  const size_t budget = 110 * 1024;
-  int wpc = (int)((budget > Ly.stage ? budget - Ly.stage : 0) / Ly.per_warp);
-  wpc = wpc < 1 ? 1 : (wpc > BS_MAXW ? BS_MAXW : wpc);
-  const size_t smem = Ly.stage + (size_t)wpc * Ly.per_warp;
   const void* fn = nbs == 4 ? (const void*)band_select_kernel<4>
                             : (nbs == 8 ? (const void*)band_select_kernel<8> : (const void*)band_select_kernel<16>);
-  cudaError_t e = xatu_raise_smem_limit(fn, smem);
+  // warps per CTA: the fewest waves of one-warp-per-k work over the GPU (resident CTAs from the occupancy
+  // calculator for each candidate), then the most warps per CTA (the staged H(R) blocks are shared by them)
+  const size_t max_smem = 227 * 1024;
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  int wmax = 1;
+  while (wmax < BS_MAXW && Ly.stage + (size_t)(wmax + 1) * Ly.per_warp <= max_smem) wmax++;
+  cudaError_t e = xatu_raise_smem_limit(fn, Ly.stage + (size_t)wmax * Ly.per_warp);
   if (e != cudaSuccess) return e;
+  int wpc = 1;
+  long long best_waves = -1;
+  for (int w = 1; w <= wmax; w++) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, w * 32, Ly.stage + (size_t)w * Ly.per_warp) !=
+            cudaSuccess ||
+        per_sm < 1)
+      continue;
+    const long long slots = (long long)per_sm * w * sms;
+    const long long waves = (bp.nk + slots - 1) / slots;
+    if (best_waves < 0 || waves <= best_waves) {
+      best_waves = waves;
+      wpc = w;
+    }
+  }
+  (void)cudaGetLastError();   // a failed occupancy query only removes its candidate
+  const size_t smem = Ly.stage + (size_t)wpc * Ly.per_warp;
   const int grid = (bp.nk + wpc - 1) / wpc;
   const int threads = wpc * 32;
   if (nbs == 4)
