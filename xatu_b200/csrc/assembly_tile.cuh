@@ -37,6 +37,21 @@ __device__ __forceinline__ void split_store(__nv_bfloat162* hi, __nv_bfloat162* 
   lo[idx] = l;
 }
 
+// Split-BF16 pair of one complex value packed as two 32-bit words: (hi.re, hi.im) and (lo.re, lo.im).  The split
+// commutes with negation (hi and lo of -x are -hi and -lo), so the conjugate of a packed value is the same words
+// with the sign bits of the imaginary halves flipped (bit 31 of each word).
+__device__ __forceinline__ uint2 split_pack(float re, float im) {
+  const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
+  __nv_bfloat162 h, l;
+  h.x = hr;
+  h.y = hi_;
+  l.x = __float2bfloat16_rn(re - __bfloat162float(hr));
+  l.y = __float2bfloat16_rn(im - __bfloat162float(hi_));
+  return make_uint2(*reinterpret_cast<const unsigned*>(&h), *reinterpret_cast<const unsigned*>(&l));
+}
+
+__device__ __forceinline__ uint2 split_conj(uint2 u) { return make_uint2(u.x ^ 0x80000000u, u.y ^ 0x80000000u); }
+
 __device__ __forceinline__ const cd* interaction_ptr(const AsmParams& p, const AsmInputs& in, int k, int k2) {
   int64_t e = interaction_entry(p, in.kpoints, in.kgrid, k, k2);
   if (e < 0) {
@@ -304,7 +319,10 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
               val.x = -d.x;
               val.y = -d.y;
             }
-            sTile[TIDX(r, cc)] = val;
+            if constexpr (MIXED)
+              reinterpret_cast<uint2*>(sTile)[TIDX(r, cc)] = split_pack((float)val.x, (float)val.y);
+            else
+              sTile[TIDX(r, cc)] = val;
           }
         }
       }
@@ -319,13 +337,22 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
     for (int t = tid; t < TR * TR; t += blockDim.x) {
       const int r = t / TR, c = t - r * TR;
       if (r > c && r < rows) {
-        const E u = sTile[TIDX(c, r)];
-        sTile[TIDX(r, c)] = E{u.x, -u.y};
+        if constexpr (MIXED) {
+          uint2* sT2 = reinterpret_cast<uint2*>(sTile);
+          sT2[TIDX(r, c)] = split_conj(sT2[TIDX(c, r)]);
+        } else {
+          const E u = sTile[TIDX(c, r)];
+          sTile[TIDX(r, c)] = E{u.x, -u.y};
+        }
       }
     }
     __syncthreads();
   }
-  if (MIXED) {
+  if constexpr (MIXED) {
+    // the tile holds the packed split-BF16 words: the planes are written without further conversion
+    const uint2* sT2 = reinterpret_cast<const uint2*>(sTile);
+    unsigned* Kh = reinterpret_cast<unsigned*>(out.Khi);
+    unsigned* Kl = reinterpret_cast<unsigned*>(out.Klo);
     constexpr int VEC = 4;                  // complex elements per 16-byte store
     constexpr int CV = (TR + VEC - 1) / VEC;
     // direct block: rows row0 + r, columns col0 + c
@@ -334,23 +361,16 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
       if (r >= rows || c >= cols) continue;
       const int64_t o = (row0 + r) * p.ldk + col0 + c;
       if (c + VEC <= cols && (o & 3) == 0) {
-        __align__(16) __nv_bfloat162 h[VEC], l[VEC];
+        uint2 u[VEC];
 #pragma unroll
-        for (int q = 0; q < VEC; q++) {
-          const E v = sTile[TIDX(r, c + q)];
-          const float re = (float)v.x, im = (float)v.y;
-          const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
-          h[q].x = hr;
-          h[q].y = hi_;
-          l[q].x = __float2bfloat16_rn(re - __bfloat162float(hr));
-          l[q].y = __float2bfloat16_rn(im - __bfloat162float(hi_));
-        }
-        *reinterpret_cast<uint4*>(out.Khi + o) = *reinterpret_cast<const uint4*>(h);
-        *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
+        for (int q = 0; q < VEC; q++) u[q] = sT2[TIDX(r, c + q)];
+        *reinterpret_cast<uint4*>(Kh + o) = make_uint4(u[0].x, u[1].x, u[2].x, u[3].x);
+        *reinterpret_cast<uint4*>(Kl + o) = make_uint4(u[0].y, u[1].y, u[2].y, u[3].y);
       } else {
         for (int q = 0; q < VEC && c + q < cols; q++) {
-          const E v = sTile[TIDX(r, c + q)];
-          split_store(out.Khi, out.Klo, o + q, (float)v.x, (float)v.y);
+          const uint2 u = sT2[TIDX(r, c + q)];
+          Kh[o + q] = u.x;
+          Kl[o + q] = u.y;
         }
       }
     }
@@ -362,23 +382,16 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         if (c >= cols || r >= rows) continue;
         const int64_t o = (col0 + c) * p.ldk + row0 + r;
         if (r + VEC <= rows && (o & 3) == 0) {
-          __align__(16) __nv_bfloat162 h[VEC], l[VEC];
+          uint2 u[VEC];
 #pragma unroll
-          for (int q = 0; q < VEC; q++) {
-            const E v = sTile[TIDX(r + q, c)];
-            const float re = (float)v.x, im = -(float)v.y;
-            const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
-            h[q].x = hr;
-            h[q].y = hi_;
-            l[q].x = __float2bfloat16_rn(re - __bfloat162float(hr));
-            l[q].y = __float2bfloat16_rn(im - __bfloat162float(hi_));
-          }
-          *reinterpret_cast<uint4*>(out.Khi + o) = *reinterpret_cast<const uint4*>(h);
-          *reinterpret_cast<uint4*>(out.Klo + o) = *reinterpret_cast<const uint4*>(l);
+          for (int q = 0; q < VEC; q++) u[q] = split_conj(sT2[TIDX(r + q, c)]);
+          *reinterpret_cast<uint4*>(Kh + o) = make_uint4(u[0].x, u[1].x, u[2].x, u[3].x);
+          *reinterpret_cast<uint4*>(Kl + o) = make_uint4(u[0].y, u[1].y, u[2].y, u[3].y);
         } else {
           for (int q = 0; q < VEC && r + q < rows; q++) {
-            const E v = sTile[TIDX(r + q, c)];
-            split_store(out.Khi, out.Klo, o + q, (float)v.x, -(float)v.y);
+            const uint2 u = split_conj(sT2[TIDX(r + q, c)]);
+            Kh[o + q] = u.x;
+            Kl[o + q] = u.y;
           }
         }
       }
