@@ -523,9 +523,19 @@ def run_engine(args):
                         "traffic": hx_traffic_per_element * N * N if hx_path == 2 else None,
                         "algorithmic_bytes_per_launch": hx_bytes, "launch_ms": hx_s * 1e3,
                         "launches_per_step": calls / len(hx_n)})
+        if hx_path == 2:
+            # tensor-core work executed per launch: three BF16 products (hi.hi, hi.lo, lo.hi) of the N x 2N real
+            # view of K with the 2N x ng operand, 2 flops per multiply-add
+            tc_flop = 3 * 2.0 * N * (2 * N) * ng
+            tensor = {"kernel": "hx_tcgen05_kernel", "executed_tflops": tc_flop / hx_s / 1e12, "peak_tflops": bf16,
+                      "frac": tc_flop / hx_s / 1e12 / bf16, "peak_source": src,
+                      "flop_per_launch": tc_flop, "arithmetic_intensity_flop_per_byte": tc_flop / hx_bytes,
+                      "ridge_flop_per_byte": bf16 * 1e3 / hbm,
+                      "note": "HBM-bound by design: the split-BF16 K is read once per block product"}
     roofline = max(kernels, key=lambda k: k["launch_ms"] * k["launches_per_step"])
 
     extra = {"davidson_iterations": statistics.median(iters), "roofline_kernels": kernels,
+             "tensor_core": tensor if calls and hx_path == 2 else None,
              "stage_ms": {"assembly": statistics.median(asm_ms), "solve": statistics.median(solve_ms)}}
     # FP64 plain path on the same system (outside the timed region): FP64 build + dense FP64 solve
     if not args.no_fp64 and rank == 0:
@@ -545,6 +555,22 @@ def run_engine(args):
         extra["fp64_path"] = {"s_per_system": t_fp64, "solver": "FP64 build + dense FP64 eigensolve (cuSOLVER)",
                               "speedup_mixed_vs_fp64": t_fp64 / t_step,
                               "max_abs_dE_eV_lowest8": float(np.abs(w_mixed - allv[:nst]).max())}
+        # oscillator strengths of the lowest states, mixed Davidson vs FP64 dense (outside the timed regions):
+        # the sum of |v|^2 over the lowest nst states is basis independent when state nst+1 is separated
+        vec_f = np.zeros((nst, N), dtype=np.complex128)
+        w_f = np.zeros(N)
+        ex._call("xatu_bse_solve", L.SOLVER_DENSE_FP64, nst, L.ptr(w_f), L.ptr(vec_f))
+        v64 = ex.excitonOscillatorStrength(vec_f.T)
+        ex._call("xatu_bse_build", L.PREC_MIXED)
+        vec_m = np.zeros((nst, N), dtype=np.complex128)
+        w_m = np.zeros(nst)
+        ex._call("xatu_bse_solve", L.SOLVER_DAVIDSON, nst, L.ptr(w_m), L.ptr(vec_m))
+        vmx = ex.excitonOscillatorStrength(vec_m.T)
+        s64 = float(np.sum(np.abs(v64) ** 2))
+        smx = float(np.sum(np.abs(vmx) ** 2))
+        extra["fp64_path"]["oscillator_strength_lowest8"] = {
+            "sum_abs2_fp64": s64, "sum_abs2_mixed": smx, "rel_err": abs(smx - s64) / max(s64, 1e-300),
+            "gap_to_next_state_eV": float(w_f[nst] - w_f[nst - 1])}
     if rank == 0 and world == 1 and not args.no_adjoint:
         extra["adjoint"] = adjoint_workload(args.adjoint_ncell, stream, hbm)
     if rank == 0 and world == 1 and not args.no_batch:
