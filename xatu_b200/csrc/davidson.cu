@@ -325,7 +325,8 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   // block = nstates plus guard vectors (at least 4), so that a state of a dense spectrum cannot drop out
   // of the block unnoticed while every residual of the block looks converged; only the first nstates must
   // converge.  The basis holds at most 4 blocks.
-  int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(4, (nstates + 3) / 4));
+  // block: the wanted states plus guard vectors (two, or a quarter of the states when more)
+  int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(2, (nstates + 3) / 4));
   bsz = std::max(bsz, nstates);
   bsz = (int)std::min<long long>(bsz, N);
   int mmax = (int)std::min<long long>(N, std::min(DAV_MAX_BASIS, 4 * bsz));
