@@ -249,12 +249,22 @@ ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* A = reinterpret_cast<cd*>(smem_raw);        // b x b row-major, lower triangle -> L
   cd* M = A + b * b;                              // L_k^{-1}, row-major
-  int* idx = reinterpret_cast<int*>(M + b * b);   // kept column indices
+  cd* Zs = M + b * b;                             // Z[0 : m + b, 0 : b], column-major (ld m + b)
+  int* idx = reinterpret_cast<int*>(Zs + (size_t)(m + b) * b);   // kept column indices
   const int lane = threadIdx.x;
+  const int mz = m + b;
+  // stage the block of Z (coalesced along each column), then G = Z[m:, :] - Z[:m, :]^H Z[:m, :] from shared memory
+  for (int t = lane; t < mz * b; t += 32) {
+    const int q = t % mz, c = t / mz;
+    Zs[t] = Z[q + (size_t)c * ldz];
+  }
+  __syncwarp();
   for (int t = lane; t < b * b; t += 32) {
     const int r = t / b, c = t - r * b;
-    cd g = Z[(m + r) + (size_t)c * ldz];
-    for (int q = 0; q < m; q++) g = g - cmulc(Z[q + (size_t)r * ldz], Z[q + (size_t)c * ldz]);
+    cd g = Zs[(m + r) + c * mz];
+    const cd* zr = Zs + r * mz;
+    const cd* zc = Zs + c * mz;
+    for (int q = 0; q < m; q++) g = g - cmulc(zr[q], zc[q]);
     A[t] = g;
   }
   __syncwarp();
@@ -309,4 +319,6 @@ ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop
   if (lane == 0) *kept = nk;
 }
 
-__host__ __device__ inline size_t ts_gram_orth_smem(int b) { return (size_t)2 * b * b * sizeof(cd) + (size_t)b * sizeof(int); }
+__host__ __device__ inline size_t ts_gram_orth_smem(int m, int b) {
+  return (size_t)(2 * b * b + (m + b) * b) * sizeof(cd) + (size_t)b * sizeof(int);
+}

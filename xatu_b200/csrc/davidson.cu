@@ -299,12 +299,12 @@ static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int n
     XATU_TRY(ts_update(ctx, t, nsel, V, m, Z, ldZ, nullptr, t, N));
   }
   XATU_TRY(ts_proj(ctx, V, m + nsel, t, nsel, N, Z, ldZ));
-  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(nsel), ctx->stream>>>(Z, ldZ, m, nsel, 1e-20, S, dkept);
+  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(m, nsel), ctx->stream>>>(Z, ldZ, m, nsel, 1e-20, S, dkept);
   ctx->launches++;
   XATU_CK_LAUNCH("ts_gram_orth_kernel");
   XATU_TRY(ts_update(ctx, t, nsel, m > 0 ? V : nullptr, m, Z, ldZ, S, X, N));
   XATU_TRY(ts_proj(ctx, X, nsel, X, nsel, N, Z, ldZ));
-  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(nsel), ctx->stream>>>(Z, ldZ, 0, nsel, 1e-24, S, dkept);
+  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(0, nsel), ctx->stream>>>(Z, ldZ, 0, nsel, 1e-24, S, dkept);
   ctx->launches++;
   XATU_CK_LAUNCH("ts_gram_orth_kernel");
   XATU_TRY(ts_update(ctx, X, nsel, nullptr, 0, nullptr, 0, S, t, N));
@@ -391,7 +391,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(xatu_raise_smem_limit((const void*)ts_proj_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_update_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_ritz_kernel, 224 * 1024));
-    XATU_CK(xatu_raise_smem_limit((const void*)ts_gram_orth_kernel, ts_gram_orth_smem(bmax)));
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_gram_orth_kernel, ts_gram_orth_smem(DAV_MAX_BASIS - bmax, bmax)));
   }
 
   // Thick-restart block Davidson on the basis V (W = H V):
