@@ -108,7 +108,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->d_adjdtable, &ctx->d_adjdVX, &ctx->d_adjAlpha, &ctx->d_adjExUW, &ctx->d_adjCbar,
                   &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG, &ctx->d_oscG,
                   &ctx->dv_part, &ctx->d_pp_X, &ctx->d_pp_A, &ctx->d_pp_B, &ctx->d_pp_C, &ctx->d_pp_D,
-                  &ctx->d_pp_P};
+                  &ctx->d_pp_P, &ctx->d_pp_E};
   for (DBuf* b : bufs) b->release();
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->blas) cublasDestroy(ctx->blas);

@@ -107,7 +107,7 @@ struct xatu_ctx {
   DBuf d_oscG;
 
   // ---------------- post-processing (postproc.cu)
-  DBuf d_pp_X, d_pp_A, d_pp_B, d_pp_C, d_pp_D, d_pp_P;
+  DBuf d_pp_X, d_pp_A, d_pp_B, d_pp_C, d_pp_D, d_pp_P, d_pp_E;
   DBuf d_adjX, d_adjdvtab, d_adjdtable, d_adjdVX, d_adjAlpha, d_adjExUW, d_adjCbar, d_adjEbar, d_adjEpart, d_adjGk,
       d_adjG;
 };

@@ -206,6 +206,18 @@ extern "C" __global__ void pp_weights_to_f_kernel(int nk, int ns, const double* 
   F[idx] = mk(kweight[(long long)s * nk + k], 0.0);
 }
 
+// E[pt][k] = exp(i sign k.d_pt) for npts points (the phase factors of the GEMM form of the transform).
+extern "C" __global__ void pp_phase_kernel(int nk, int npts, const double* __restrict__ kpts,
+                                           const double* __restrict__ pts, double sign, cd* __restrict__ E) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)nk * npts) return;
+  const int pt = (int)(idx / nk), k = (int)(idx - (long long)pt * nk);
+  const double x = kpts[3 * k] * pts[3 * pt] + kpts[3 * k + 1] * pts[3 * pt + 1] + kpts[3 * k + 2] * pts[3 * pt + 2];
+  double sn, cs;
+  sincos(x, &sn, &cs);
+  E[idx] = mk(cs, sign * sn);
+}
+
 #define DFT_TK 16    // k points per shared-memory stage
 
 // part[z][pt][p] = sum_{k in split z} exp(i sign k.d_pt) F[k][p].  A CTA covers 8*CPW points x PT*NPL pairs:
@@ -453,6 +465,7 @@ static long long pp_dim(const xatu_ctx* ctx) { return (long long)ctx->nk * ctx->
 //   d_pp_X  coefficients (N x ns)          d_pp_A  pair table F / velocity matrix elements
 //   d_pp_B  per-k weights, points, output  d_pp_C  per-k partials of the state reductions
 //   d_pp_D  state summaries / absorption   d_pp_P  split-k partials of the k-space transforms
+//   d_pp_E  phase matrix of the GEMM form of the transform
 
 static size_t pp_obs_bytes_c(const xatu_ctx* ctx, int ns) {
   return (size_t)ns * ctx->nk * (OBS_PARTS + 1) * sizeof(double) + (size_t)ctx->norb * sizeof(double);
@@ -540,7 +553,15 @@ extern "C" xatu_status xatu_state_observables(xatu_ctx* ctx, int nstates, const 
 struct KdftPlan {
   int PT, NPL, CPW, nsplit, kchunk;
   dim3 grid;
+  int gemm;    // 1: phase matrix E (chunks of `chunk` points) times F with cuBLAS ZGEMM
+  int chunk;
 };
+
+// From this many pairs on, the transform is a plain complex GEMM G = E F: the phase matrix of a chunk of
+// points is formed once (pp_phase_kernel) and multiplied by cuBLAS ZGEMM (FP64 tensor cores), which sustains
+// a higher FP64 rate than the fused kernel; the chunk keeps E under the byte bound.
+#define PP_GEMM_MIN_PAIRS 64
+#define PP_E_BUDGET (256ull << 20)
 
 #define PP_KDFT_VARIANTS(X) \
   X(1, 1, 8) X(2, 1, 8) X(4, 1, 8) X(8, 1, 8) X(16, 1, 8) X(32, 1, 8) X(32, 2, 8) X(32, 4, 4)
@@ -564,6 +585,17 @@ static size_t pp_kdft_smem_of(int PT, int NPL, int CPW) {
 static KdftPlan pp_kdft_plan(const xatu_ctx* ctx, int P, int npts) {
   KdftPlan pl;
   const int nk = ctx->nk;
+  pl.gemm = 0;
+  pl.chunk = 0;
+  if (P >= PP_GEMM_MIN_PAIRS) {
+    pl.gemm = 1;
+    pl.PT = pl.NPL = pl.CPW = 0;
+    pl.nsplit = 1;
+    pl.kchunk = nk;
+    pl.chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)npts, PP_E_BUDGET / ((size_t)nk * sizeof(cd))));
+    pl.grid = dim3(1, 1, 1);
+    return pl;
+  }
   pl.PT = 1;
   while (pl.PT < 32 && pl.PT < P) pl.PT <<= 1;
   pl.NPL = (P >= 128) ? 4 : (P > 32) ? 2 : 1;
@@ -600,6 +632,9 @@ static KdftPlan pp_kdft_plan(const xatu_ctx* ctx, int P, int npts) {
 }
 
 static size_t pp_kdft_bytes(const KdftPlan& pl, int P, int npts) { return (size_t)pl.nsplit * npts * P * sizeof(cd); }
+static size_t pp_kdft_ebytes(const xatu_ctx* ctx, const KdftPlan& pl) {
+  return pl.gemm ? (size_t)pl.chunk * ctx->nk * sizeof(cd) : 0;
+}
 
 // d_pp_P[z][pt][p] = sum_{k in split z} exp(i sign k.d_pt) F[k][p] (d_pp_P sized by the caller).
 static xatu_status pp_kdft(xatu_ctx* ctx, const KdftPlan& pl, const cd* F, int P, int npts, const double* dpts,
@@ -607,6 +642,28 @@ static xatu_status pp_kdft(xatu_ctx* ctx, const KdftPlan& pl, const cd* F, int P
   const int nk = ctx->nk;
   const double* kp = ctx->d_kpoints.as<double>();
   cd* part = ctx->d_pp_P.as<cd>();
+  if (pl.gemm) {
+    // column-major view: G (P x npts, ld P) = F (P x nk, ld P) E (nk x npts, ld nk)
+    if (!ctx->blas && cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS)
+      return xatu_fail(ctx, XATU_ERR_CUDA, "cublasCreate failed");
+    if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS)
+      return xatu_fail(ctx, XATU_ERR_CUDA, "cublasSetStream failed");
+    cd* E = ctx->d_pp_E.as<cd>();
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    for (int c0 = 0; c0 < npts; c0 += pl.chunk) {
+      const int nc = std::min(pl.chunk, npts - c0);
+      const long long tot = (long long)nk * nc;
+      pp_phase_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(nk, nc, kp, dpts + 3 * (size_t)c0, sign,
+                                                                              E);
+      ctx->launches++;
+      XATU_CK_LAUNCH("pp_phase_kernel");
+      if (cublasZgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, P, nc, nk, &one,
+                      reinterpret_cast<const cuDoubleComplex*>(F), P, reinterpret_cast<const cuDoubleComplex*>(E), nk,
+                      &zero, reinterpret_cast<cuDoubleComplex*>(part + (size_t)c0 * P), P) != CUBLAS_STATUS_SUCCESS)
+        return xatu_fail(ctx, XATU_ERR_CUDA, "cublasZgemm (k-space transform) failed");
+    }
+    return XATU_OK;
+  }
   const dim3 g = pl.grid;
   const int kc = pl.kchunk;
   const size_t sm = pp_kdft_smem_of(pl.PT, pl.NPL, pl.CPW);
@@ -649,8 +706,9 @@ extern "C" xatu_status xatu_realspace_amplitude(xatu_ctx* ctx, int nstates, cons
   XATU_CK(ctx->d_pp_X.ensure((size_t)N * group * sizeof(cd)));
   XATU_CK(ctx->d_pp_A.ensure(per_state * group));
   XATU_CK(ctx->d_pp_B.ensure((size_t)ncells * 3 * sizeof(double) + group * ncells * natoms * sizeof(double)));
-  // later (smaller) groups need no more partials than the first
+  // later (smaller) groups need no more partials (nor phase matrix) than the first
   XATU_CK(ctx->d_pp_P.ensure(pp_kdft_bytes(pl0, P0, ncells)));
+  XATU_CK(ctx->d_pp_E.ensure(pp_kdft_ebytes(ctx, pl0)));
   double* dpts = ctx->d_pp_B.as<double>();
   double* dout = dpts + (size_t)ncells * 3;
   XATU_CK(cudaMemcpyAsync(dpts, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -658,7 +716,7 @@ extern "C" xatu_status xatu_realspace_amplitude(xatu_ctx* ctx, int nstates, cons
     const int ns = std::min((int)group, nstates - s0);
     const int P = ns * norb * nho;
     const KdftPlan pl = pp_kdft_plan(ctx, P, ncells);
-    if (pp_kdft_bytes(pl, P, ncells) > ctx->d_pp_P.bytes)
+    if (pp_kdft_bytes(pl, P, ncells) > ctx->d_pp_P.bytes || pp_kdft_ebytes(ctx, pl) > ctx->d_pp_E.bytes)
       return xatu_fail(ctx, XATU_ERR_INVALID, "internal: k-space transform partials exceed their buffer");
     XATU_CK(cudaMemcpyAsync(ctx->d_pp_X.p, eigvec + (size_t)2 * N * s0, (size_t)N * ns * sizeof(cd),
                             cudaMemcpyHostToDevice, ctx->stream));
@@ -698,6 +756,7 @@ extern "C" xatu_status xatu_envelope_ft(xatu_ctx* ctx, int nstates, const double
   XATU_CK(ctx->d_pp_A.ensure((size_t)nk * nstates * sizeof(cd)));
   XATU_CK(ctx->d_pp_D.ensure((size_t)npoints * 3 * sizeof(double) + (size_t)nstates * npoints * sizeof(double)));
   XATU_CK(ctx->d_pp_P.ensure(pp_kdft_bytes(pl, nstates, npoints)));
+  XATU_CK(ctx->d_pp_E.ensure(pp_kdft_ebytes(ctx, pl)));
   double* dpts = ctx->d_pp_D.as<double>();
   double* dout = dpts + (size_t)npoints * 3;
   st = pp_state_obs(ctx, nstates, eigvec, false, false);
