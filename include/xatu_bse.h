@@ -232,7 +232,9 @@ enum {
      sigma_ex  nw x 9 real: sum_n Re(pi/(nk vcell) conj(V_i,n) V_j,n / E_n) broadening(w - E_n), i, j < 2
                (the other entries 0, as in the reference), over the nstates given states.
      vme_ex    optional, 3 x nstates complex column-major: their velocity matrix elements (atomic units).
-   eigval: nstates exciton energies (eV).  nstates = 0 computes the single-particle part only. */
+   eigval: nstates exciton energies (eV).  nstates = 0 computes the single-particle part only.  vcell is
+   |a1 x a2| in bohr^2 as in skubo_w.f90:69-71; it is zero for a one-dimensional lattice, where the reference
+   divides by it and so does this entry (infinite or NaN values). */
 xatu_status xatu_absorption(xatu_ctx *ctx, int nstates, const double *eigval, const double *eigvec, double w0,
                             double wrange, int nw, double eta, int broadening, double *sigma_sp, double *sigma_ex,
                             double *vme_ex);
