@@ -503,8 +503,8 @@ def run_engine(args):
     #    and adds into Y (N x 2b FP32).
     hbm, bf16, src = peaks()
     # DRAM traffic of the K.X product per launch, from an ncu capture of the same kernel at N = 5184
-    # (k mesh 36 x 36, K = 215 MB > L2; dram__bytes_read.sum + dram__bytes_write.sum = 220.4 MB per launch,
-    # profiles/hx_tcgen05_traffic.md), scaled by N^2 (the reads stream K once, so traffic grows with it)
+    # (k mesh 36 x 36, K = 215 MB > L2; dram__bytes_read.sum + dram__bytes_write.sum = 220.4 MB per launch),
+    # scaled by N^2 (the reads stream K once, so traffic grows with it)
     hx_traffic_per_element = (219.78e6 + 0.61e6) / 5184.0 ** 2
     asm_s = statistics.median(asm_ms) / 1e3
     asm_bytes = N * N * 8 + N * 8

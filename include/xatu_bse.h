@@ -14,8 +14,8 @@
  *   - Complex numbers are interleaved (re, im) doubles.
  *   - Matrices are row-major unless stated otherwise.  The tight-binding
  *     matrices H(R) are given per cell as [R][row][col] (an Armadillo cube
- *     slice is column-major; a caller holding one passes its transpose, see
- *     INTEGRATION.md).
+ *     slice is column-major; a caller holding one passes each slice
+ *     transposed).
  *   - Units: Angstrom and eV, as in the reference.
  *   - Every call returns a status; xatu_last_error() gives the message of the
  *     last failing call on that context.  No call throws, exits or spins
