@@ -232,3 +232,23 @@ def test_error_paths():
         ex.diagonalize("diag", 3)          # dense solver needs the FP64 build
     with pytest.raises(ValueError):
         ex.setMode("momentum")
+
+
+@pytest.mark.parametrize("ncell,nstates", [(6, 8), (5, 12)])
+def test_davidson_basis_covers_small_space(ncell, nstates):
+    """FP64 Davidson on a space barely larger than its basis (N = 36 or 25 with blocks of 10-16) and a tight
+    tolerance: the corrections become linearly dependent on the basis, the orthonormalisation drops
+    directions (left as zero columns and parked on the device), and the solve still ends with the exact
+    lowest eigenpairs."""
+    cfg = model_config("hBN.model")
+    ex, orc = _pair(cfg, ncell, 1, [1, 1, 10])
+    ex.BShamiltonian("fp64")
+    ex.davidsonConfig(1e-10, 200, 0)
+    res = ex.diagonalize("davidson", nstates)
+    Ho = orc.bs_hamiltonian()
+    w = np.linalg.eigvalsh(Ho)[:nstates]
+    assert np.abs(res.eigval - w).max() < 1e-8
+    for s in range(nstates):
+        x = res.eigvec[:, s]
+        assert abs(np.vdot(x, x) - 1) < 1e-8
+        assert np.abs(Ho @ x - w[s] * x).max() < 1e-6

@@ -77,6 +77,38 @@ __global__ void dav_finish_w_kernel(const float2* __restrict__ Y, const double* 
 }
 
 // T (column-major, ld) : fill T[m0:m, 0:m0] = conj(T[0:m0, m0:m])^T and make the new block Hermitian.
+// Columns of the new block that the orthonormalisation dropped are exact zero vectors (and so are their
+// W = H V columns): their rows and columns of T are zero.  Their diagonal is set above a Gershgorin bound of
+// the kept part, so they stay decoupled and never enter the lowest Ritz pairs (their Ritz coefficients
+// multiply zero columns).  The kept count is copied next to the Ritz values for the host's read-back.
+__global__ void dav_dead_kernel(cd* T, int ld, int m, int m0, const int* __restrict__ kept, double* kept_out) {
+  const int nnew = m - m0;
+  const int kc = min(max(*kept, 0), nnew);
+  if (threadIdx.x == 0) *kept_out = (double)kc;
+  if (kc >= nnew) return;   // uniform over the CTA
+  const int live = m0 + kc;
+  __shared__ double red[32];
+  double bnd = -INFINITY;
+  for (int r = threadIdx.x; r < live; r += blockDim.x) {
+    double sum = T[r + (long long)r * ld].x;
+    for (int c = 0; c < live; c++)
+      if (c != r) {
+        const cd v = T[r + (long long)c * ld];
+        sum += sqrt(v.x * v.x + v.y * v.y);
+      }
+    bnd = fmax(bnd, sum);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bnd = fmax(bnd, __shfl_xor_sync(0xffffffffu, bnd, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bnd;
+  __syncthreads();
+  double b = -INFINITY;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) b = fmax(b, red[w]);
+  if (!(b > -INFINITY)) b = 0.0;
+  const double shift = b + fmax(1.0, fabs(b));
+  for (int j = live + threadIdx.x; j < m; j += blockDim.x) T[j + (long long)j * ld] = mk(shift, 0.0);
+}
+
 __global__ void dav_hermitize_kernel(cd* T, int ld, int m, int m0) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int nnew = m - m0;
@@ -284,9 +316,9 @@ static xatu_status ts_update(xatu_ctx* ctx, const cd* In, int b, const cd* A, in
 //   t <- t - V (V^H t);
 //   Z = [V t]^H t: C = V^H t, G = t^H t - C^H C; Cholesky of G with dropping -> S;  X = (t - V C) S;
 //   G = X^H X -> S (second Cholesky pass, absolute threshold);  t <- X S.
-// The kept directions end in V[:, m : m + kept], the rest of the block is zero; `kept` is read back (the
-// one synchronisation of this step).
-static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int nsel, int* kept) {
+// The kept directions end in V[:, m : m + kept] and the rest of the block is zero; kept stays on the device
+// (dav_dead_kernel of the next step parks the zero columns and hands the count to the host's read-back).
+static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int nsel) {
   cd* V = ctx->dv_V.as<cd>();
   cd* t = V + (long long)m * N;
   cd* X = ctx->dv_tmp.as<cd>();
@@ -308,9 +340,6 @@ static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int n
   ctx->launches++;
   XATU_CK_LAUNCH("ts_gram_orth_kernel");
   XATU_TRY(ts_update(ctx, X, nsel, nullptr, 0, nullptr, 0, S, t, N));
-  XATU_CK(cudaMemcpyAsync(ctx->h_small, dkept, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  XATU_CK(cudaStreamSynchronize(ctx->stream));
-  *kept = *reinterpret_cast<int*>(ctx->h_small);
   return XATU_OK;
 }
 
@@ -322,10 +351,9 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   cublasSetStream(ctx->blas, ctx->stream);
   cublasSetPointerMode(ctx->blas, CUBLAS_POINTER_MODE_HOST);
   const bool mixed = ctx->built_prec == XATU_PREC_MIXED;
-  // block = nstates plus guard vectors (at least 4), so that a state of a dense spectrum cannot drop out
-  // of the block unnoticed while every residual of the block looks converged; only the first nstates must
-  // converge.  The basis holds at most 4 blocks.
-  // block: the wanted states plus guard vectors (two, or a quarter of the states when more)
+  // block = nstates plus guard vectors (two, or a quarter of the states when more), so that a state of a dense
+  // spectrum cannot drop out of the block unnoticed while every residual of the block looks converged; only
+  // the first nstates must converge.  The basis holds at most 4 blocks.
   int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(2, (nstates + 3) / 4));
   bsz = std::max(bsz, nstates);
   bsz = (int)std::min<long long>(bsz, N);
@@ -357,6 +385,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   double* theta = ctx->dv_norm.as<double>();            // [0, 256)
   double* norms = theta + 256;                          // [256, 512)
   int* sel_dev = reinterpret_cast<int*>(theta + 512);   // ints
+  int* dkept = reinterpret_cast<int*>(theta + 1024);    // kept columns of the newest block (ts_gram_orth_kernel)
   double* diagH = ctx->dv_diagH.as<double>();
   const int threads = 256;
   // diagonal of H
@@ -379,6 +408,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   std::partial_sort(order.begin(), order.begin() + bsz, order.end(),
                     [&](int a, int b) { return hdiag[a] < hdiag[b] || (hdiag[a] == hdiag[b] && a < b); });
   XATU_CK(cudaMemcpyAsync(sel_dev, order.data(), bsz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  XATU_CK(cudaMemcpyAsync(dkept, &bsz, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   {
     const long long tot = N * bsz;
     dav_unit_vectors_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(V, N, 0, sel_dev, bsz);
@@ -399,6 +429,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   //   U = V Y, WU = W Y, residuals WU - U theta;  corrections appended after orthonormalisation;
   //   restart: V <- U, W <- WU, T <- diag(theta).
   int m0 = 0, m = bsz;
+  int dead = 0;   // zero columns in V[:, 0 : m] (directions the orthonormalisation dropped)
   int it = 0;
   bool converged = false;
   std::vector<double> h_theta(ldT), h_norm(bsz);
@@ -420,6 +451,9 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       dav_hermitize_kernel<<<(tot + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, m0);
       ctx->launches++;
       XATU_CK(cudaGetLastError());
+      dav_dead_kernel<<<1, 128, 0, ctx->stream>>>(T, ldT, m, m0, dkept, theta + 769);
+      ctx->launches++;
+      XATU_CK_LAUNCH("dav_dead_kernel");
     }
     // 3. Rayleigh-Ritz: the lowest nritz eigenpairs of T
     const int nritz = std::min(bsz, m);
@@ -443,8 +477,9 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK_LAUNCH("ts_sum_kernel");
     }
-    // one read-back: theta [0, 256), residual norms [256, 512), status word at 768
-    XATU_CK(cudaMemcpyAsync(ctx->h_small, theta, 769 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    // one read-back: theta [0, 256), residual norms [256, 512), status word at 768, kept columns of the
+    // newest block at 769
+    XATU_CK(cudaMemcpyAsync(ctx->h_small, theta, 770 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     XATU_CK(cudaStreamSynchronize(ctx->stream));
     xatu_hx_collect(ctx);
     {
@@ -453,6 +488,8 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       for (int c = 0; c < nritz; c++) h_norm[c] = std::sqrt(hb[256 + 2 * c]);
     }
     const int st = (int)reinterpret_cast<const double*>(ctx->h_small)[768];
+    const int kept_new = (int)reinterpret_cast<const double*>(ctx->h_small)[769];
+    dead += (m - m0) - kept_new;   // zero columns of the newest block
     if (st) {
       cudaMemsetAsync(ctx->d_status.p, 0, sizeof(int), ctx->stream);
       return xatu_fail(ctx, XATU_ERR_NOT_CONVERGED, "Davidson: Rayleigh-Ritz or K.X stage reported an error");
@@ -464,10 +501,11 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
         return xatu_fail(ctx, XATU_ERR_NUMERIC, "Davidson: non-finite Ritz value or residual");
     ctx->dav_iters = it + 1;
     ctx->dav_maxres = maxres;
-    if (maxres < tol || m >= N) {
+    if (maxres < tol || m - dead >= N) {
       converged = true;
       break;
     }
+    if (it > 0 && kept_new == 0) break;   // the last corrections added no direction
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     if (el > wall_cap_s) break;
     // 5. correction targets: unconverged among the lowest Ritz pairs
@@ -483,6 +521,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK(cudaGetLastError());
       m = nritz;
+      dead = 0;
       if (m + nsel > mmax) nsel = mmax - m;
     }
     if (nsel <= 0) break;
@@ -494,11 +533,9 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK_LAUNCH("ts_gather_kernel");
     }
-    int kept = 0;
-    XATU_TRY(orthonormalize_block(ctx, N, m, nsel, &kept));
-    if (kept == 0) break;
+    XATU_TRY(orthonormalize_block(ctx, N, m, nsel));
     m0 = m;
-    m += kept;
+    m += nsel;   // dropped directions stay as zero columns, parked by dav_dead_kernel
   }
   // results: the Ritz vectors of the last Rayleigh-Ritz step
   std::copy(h_theta.begin(), h_theta.begin() + nstates, eigval);
