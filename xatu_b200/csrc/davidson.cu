@@ -351,10 +351,10 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   cublasSetStream(ctx->blas, ctx->stream);
   cublasSetPointerMode(ctx->blas, CUBLAS_POINTER_MODE_HOST);
   const bool mixed = ctx->built_prec == XATU_PREC_MIXED;
-  // block = nstates plus guard vectors (two, or a quarter of the states when more), so that a state of a dense
+  // block = nstates plus guard vectors (two, or an eighth of the states when more), so that a state of a dense
   // spectrum cannot drop out of the block unnoticed while every residual of the block looks converged; only
   // the first nstates must converge.  The basis holds at most 4 blocks.
-  int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(2, (nstates + 3) / 4));
+  int bsz = ctx->dav_block > 0 ? ctx->dav_block : std::max(8, nstates + std::max(2, (nstates + 7) / 8));
   bsz = std::max(bsz, nstates);
   bsz = (int)std::min<long long>(bsz, N);
   int mmax = (int)std::min<long long>(N, std::min(DAV_MAX_BASIS, 4 * bsz));
