@@ -155,7 +155,10 @@ xatu_status xatu_bse_dim(const xatu_ctx *ctx, int64_t *n);
    (diagonal band term + split-BF16 kernel). */
 xatu_status xatu_bse_copy_to_host(xatu_ctx *ctx, double *H);
 /* Device pointer and layout of the assembled matrix (row-major complex128 for FP64; for MIXED the two
-   split-BF16 planes hi and lo, each N x N complex bf16, and the FP64 diagonal). */
+   split-BF16 planes hi and lo, each N x ldk complex bf16 with ldk = N rounded up to a multiple of 4, and the
+   FP64 diagonal).  The MIXED planes hold the Hermitian kernel's upper block triangle only: with blocks of
+   128 x 128 elements, element (r, c) is stored when c / 128 >= r / 128 (the diagonal blocks in full); any
+   other element is the conjugate of its mirror (c, r). */
 xatu_status xatu_bse_device_buffers(xatu_ctx *ctx, void **h_or_hi, void **lo, void **diag);
 
 /* ------------------------------------------------------------------ diagonalize (ExcitonTB.cpp:930-972) */
@@ -320,13 +323,16 @@ xatu_status xatu_selftest_small_eigh(int device, int m, int k, const double *T, 
    (nearly) all of the GPU's memory in their own pool, and caller-written iterative eigensolvers that request
    the product thousands of times and cannot afford a cudaMalloc/cudaFree (device-wide synchronisation) per
    request.  All arguments are device pointers owned by the caller: k_hi, k_lo, diag as returned by
-   xatu_bse_device_buffers for XATU_PREC_MIXED (n x ldk complex bf16 planes, ldk a multiple of 4), x and y
-   n x nvec complex128, column-major, 16-byte aligned.  Limits: n <= 16384, nvec <= 16; larger sizes return
-   XATU_ERR_UNSUPPORTED with a message on stderr.  Scratch is one static 6 MB device array per GPU that loads
-   the library, held until the process exits; the first call on a device looks up its address (do that first
-   call before any stream capture).  Every call shares that array and leaves its contents behind, so calls
-   that overlap on the GPU (other streams, other host threads) race.  Runs on `stream` (cudaStream_t, NULL =
-   legacy default stream) and waits for it before returning. */
+   xatu_bse_device_buffers for XATU_PREC_MIXED (n x ldk complex bf16 planes, ldk a multiple of 4, upper block
+   triangle stored), x and y n x nvec complex128, column-major, 16-byte aligned.  Limits: n <= 16384,
+   nvec <= 16; larger sizes return XATU_ERR_UNSUPPORTED with a message on stderr.  Scratch is one static 8 MB
+   device array per GPU that loads
+   the library, held until the process exits; the first call on a device (and the first after that device's
+   context was recreated) looks up its address (do that first call before any stream capture).  Every call
+   shares that array and leaves its contents behind, so calls that overlap on the GPU (other streams, other
+   host threads) race.  Runs on `stream` (cudaStream_t, NULL = legacy default stream) and waits for it before
+   returning, to read its status word: on a stream that is being captured it does nothing and returns
+   XATU_ERR_STATE.  A tensor-core pipeline wait that timed out returns XATU_ERR_NOT_CONVERGED. */
 xatu_status xatu_hx_noalloc(const void *k_hi, const void *k_lo, const double *diag, int64_t n, int64_t ldk, int nvec,
                             const double *x, double *y, void *stream);
 

@@ -434,17 +434,28 @@ class OracleExciton:
         raise ValueError(f"unsupported method {method}")
 
 
-def davidson_method(mat: np.ndarray, neigval: int, tol: float = 1e-8):
-    """davidson_method (davidson.cpp:5-60), restated in numpy (QR by LAPACK geqrf)."""
+def davidson_method(mat: np.ndarray, neigval: int, tol: float = 1e-8, max_seconds: float = None,
+                    stats: dict = None, check_hermitian: bool = True):
+    """davidson_method (davidson.cpp:5-60), restated in numpy (QR by LAPACK geqrf).
+
+    max_seconds (not in the reference): stop after the iteration that crosses this wall time, for bounded CPU
+    timings; ``stats`` (a dict) then receives the iteration count and whether the eigenvalues converged.
+    check_hermitian=False skips the reference's O(N^2) Hermiticity check for matrices built Hermitian."""
+    import time as _time
+    t_start = _time.perf_counter()
     n = mat.shape[0]
     max_it = n // 2
     k = neigval * 2
-    if not np.allclose(mat, mat.conj().T):
+    if check_hermitian and not np.allclose(mat, mat.conj().T):
         raise ValueError("davidson_method: provided matrix must be hermitian")
     guess = np.eye(n, k, dtype=np.complex128)
     aux = np.ones(neigval)
     eigval = eigvec = None
+    if stats is not None:
+        stats.update(iterations=0, converged=False)
     for i in range(max_it):
+        if stats is not None:
+            stats["iterations"] = i + 1
         Qm, _ = np.linalg.qr(guess)
         proj = Qm.conj().T @ mat @ Qm
         eigval, eigvec = np.linalg.eigh(proj)
@@ -455,9 +466,13 @@ def davidson_method(mat: np.ndarray, neigval: int, tol: float = 1e-8):
             cols.append((w / (eigval[j] - mat[j, j]))[:, None])
         Qm = np.concatenate(cols, axis=1)
         if np.linalg.norm(eigval[:neigval] - aux) < tol:
+            if stats is not None:
+                stats["converged"] = True
             break
         aux = eigval[:neigval].copy()
         guess = Qm
+        if max_seconds is not None and _time.perf_counter() - t_start > max_seconds:
+            break
     return eigval[:neigval], eigvec
 
 

@@ -97,4 +97,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_fixtures.py <path of the xatu source tree>")
+    main(sys.argv[1])

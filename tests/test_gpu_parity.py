@@ -73,18 +73,39 @@ def test_fp64_matrix_parity_shared_bands(case):
     assert np.array_equal(H, H.conj().T)
 
 
+@pytest.mark.parametrize("path", ["fp64-diag", "mixed-davidson"])
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
-def test_energies_device_bands_dense(case):
-    """Whole device path (bands, tables, FP64 build, dense FP64 solve) against the reference goldens."""
+def test_energies_device_bands(case, path):
+    """Whole device path (bands, tables, build, solve) against the reference goldens (tests.cpp:150-279,
+    547-774), each case at its own tolerance, through two paths: the FP64 build with the dense FP64 solve,
+    and the path the benchmark times, the split-BF16 build with the tcgen05 block Davidson.
+
+    Degeneracies: the FP64 path groups eigenvalues as the reference does (detectDegeneracies(.., 6): closer
+    than 1e-6 eV).  The mixed path lifts exact degeneracies slightly (split-BF16 storage of K, Davidson
+    residual 1e-4 eV), so it is checked without a grouping threshold: its ascending eigenvalues are taken in
+    order, each golden level (E, d) consuming the next d of them, every one within the golden tolerance of E.
+    The Davidson solves two states more than the case checks, so that the states of a level are all there."""
     cfg = model_config(case["model"])
     kw = case_kwargs(case)
     ex = engine_exciton(cfg, case["ncell"], case["nbands"], case["params"], **kw)
-    ex.BShamiltonian("fp64")
-    res = ex.diagonalize("diag", case["nstates"])
-    pairs = detect_degeneracies(res.eigval, case["nstates"], 6)
-    for (e, d), (ee, dd) in zip(pairs, case["expected"]):
-        assert e == pytest.approx(ee, abs=case["tol"])
-        assert d == dd
+    n = case["nstates"]
+    if path == "fp64-diag":
+        ex.BShamiltonian("fp64")
+        res = ex.diagonalize("diag", n)
+        pairs = detect_degeneracies(res.eigval, n, 6)
+        for (e, d), (ee, dd) in zip(pairs, case["expected"]):
+            assert e == pytest.approx(ee, abs=case["tol"])
+            assert d == dd
+    else:
+        ex.BShamiltonian("mixed")
+        w = ex.diagonalize("davidson", n + 2).eigval
+        i = 0
+        for ee, dd in case["expected"]:
+            if i + dd > len(w):
+                break
+            got = w[i:i + dd]
+            assert np.abs(got - ee).max() <= case["tol"], (case["name"], ee, dd, w)
+            i += dd
 
 
 def test_mixed_build_parity():
@@ -252,3 +273,51 @@ def test_davidson_basis_covers_small_space(ncell, nstates):
         x = res.eigvec[:, s]
         assert abs(np.vdot(x, x) - 1) < 1e-8
         assert np.abs(Ho @ x - w[s] * x).max() < 1e-6
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", FP64_TOL), ("mixed", MIXED_TOL)])
+def test_headline_size_rows_match_oracle(precision, tol):
+    """The benchmark's system at full size (22-orbital model, Nk = 60 x 60, 2v + 2c, N = 14400, real-space
+    Keldysh r0 = 40, eps = (1, 4.5)): 256 rows spread over the matrix, built by the engine with the oracle's
+    band stacks uploaded, against the oracle's element loop for the same rows (orc_bse_build_rows, the
+    restatement of ExcitonTB.cpp:857-917).  The diagonal carries the band energies on one side only and is
+    compared separately through the band-energy term."""
+    from xatu_b200.synthetic import synthetic_hexagonal
+    cfg = synthetic_hexagonal(seed=1234)
+    ex, orc = _pair(cfg, 60, 2, [1.0, 4.5, 40.0])
+    assert orc.N == 14400
+    ex.upload_bands(orc.eigval, orc.eigvec)
+    ex.BShamiltonian(precision)
+    H = ex.HBS
+    rows = np.unique(np.linspace(0, orc.N - 2, 256).astype(int))
+    assert len(rows) == 256
+    scale, err, derr = 0.0, 0.0, 0.0
+    for r in rows:
+        o = orc.bs_rows(int(r), int(r) + 1)[0]
+        e = H[r]
+        scale = max(scale, float(np.abs(o[r + 1:]).max()))
+        err = max(err, float(np.abs(e[r + 1:] - o[r + 1:]).max()))
+        # diagonal: H_ii = scissor + E_c - E_v - (D - X)_ii
+        ki, v, c = orc.basis_k[r], orc.basis_v[r], orc.basis_c[r]
+        band = orc.scissor + orc.eigvalQ[ki, c] - orc.eigval[ki, v]
+        derr = max(derr, abs(e[r].real - (band + o[r].real)))
+    assert err / scale < tol, (err, scale)
+    assert derr < tol * scale, (derr, scale)
+    # Hermitian: the lower triangle is the conjugate of the upper one
+    blk = H[rows[:16]][:, rows[:16]]
+    assert np.abs(blk - blk.conj().T).max() <= 1e-15 * scale
+
+
+def test_reciprocal_exchange_16_states_vs_oracle():
+    """The physics of the reciprocal-space workload (22-orbital model, nG = 5 x 5 = 25 G vectors, direct +
+    exchange, 2v + 2c, lowest 16 states) at a mesh the oracle solves densely (Nk = 24 x 24, N = 2304):
+    whole device path, mixed build + Davidson, against the oracle's dense eigenvalues."""
+    from xatu_b200.synthetic import synthetic_hexagonal
+    cfg = synthetic_hexagonal(seed=1234)
+    kw = dict(mode="reciprocalspace", nG=5, exchange=True)
+    ex, orc = _pair(cfg, 24, 2, [1.0, 4.5, 40.0], **kw)
+    assert orc.G.shape[0] == 25
+    ex.BShamiltonian("mixed")
+    res = ex.diagonalize("davidson", 16)
+    w = np.linalg.eigvalsh(orc.bs_hamiltonian())[:16]
+    assert np.abs(res.eigval - w).max() < ENERGY_TOL

@@ -20,6 +20,29 @@ import numpy as np
 from . import _lib as L
 
 
+def member_cost(nk: int, nv: int, nc: int) -> int:
+    """Work of one member, in units of matrix elements: the assembly writes and every K.X product reads
+    the N x N kernel, N = nk * nv * nc."""
+    n = nk * nv * nc
+    return n * n
+
+
+def shard_members(costs, world: int):
+    """Partition of batch members over `world` ranks with balanced total cost: members in decreasing cost
+    (ties by index), each to the rank with the least cost so far (ties to the lowest rank).  Deterministic,
+    so every rank computes the same partition from the same list without communicating.  Returns one
+    sorted list of member indices per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(costs)), key=lambda j: (-costs[j], j)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
 class ExcitonBatch:
     def __init__(self, device: int = 0):
         self.device = device

@@ -104,7 +104,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status,
                   &ctx->d_work, &ctx->dv_V, &ctx->dv_W, &ctx->dv_T, &ctx->dv_Y, &ctx->dv_U, &ctx->dv_R,
                   &ctx->dv_X, &ctx->dv_Yf, &ctx->dv_G, &ctx->dv_tmp, &ctx->dv_diagH, &ctx->dv_small,
-                  &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo, &ctx->d_adjX, &ctx->d_adjdvtab,
+                  &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo, &ctx->dv_Uhi, &ctx->dv_Ulo, &ctx->d_adjX, &ctx->d_adjdvtab,
                   &ctx->d_adjdtable, &ctx->d_adjdVX, &ctx->d_adjAlpha, &ctx->d_adjExUW, &ctx->d_adjCbar,
                   &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG, &ctx->d_oscG,
                   &ctx->dv_part, &ctx->d_pp_X, &ctx->d_pp_A, &ctx->d_pp_B, &ctx->d_pp_C, &ctx->d_pp_D,
@@ -736,9 +736,13 @@ __global__ void expand_mixed_kernel(const __nv_bfloat162* __restrict__ hi, const
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const long long r = row0 + t / N, c = t % N;
-    const __nv_bfloat162 h = hi[r * ldk + c], l = lo[r * ldk + c];
+    // the kernel planes hold the upper block triangle; the rest is the conjugate of its mirror
+    const bool st = xatu_kstored(r, c);
+    const long long o = st ? r * ldk + c : c * ldk + r;
+    const __nv_bfloat162 h = hi[o], l = lo[o];
     double re = (double)__bfloat162float(h.x) + (double)__bfloat162float(l.x);
-    const double im = (double)__bfloat162float(h.y) + (double)__bfloat162float(l.y);
+    double im = (double)__bfloat162float(h.y) + (double)__bfloat162float(l.y);
+    if (!st) im = -im;
     if (r == c) re += diag[r];
     out[t] = mk(re, im);
   }

@@ -17,15 +17,17 @@
 // the reference) from band coefficients staged in shared memory
 // ([band][orbital][k] layout so the k' threads of a warp read consecutive
 // words).  Only tiles with kblock <= kblock' are launched; the mirror block is
-// written as the conjugate transpose, so H is exactly Hermitian.
+// written as the conjugate transpose, so H is exactly Hermitian.  The mixed
+// build stores only the upper block triangle of K (blocks of XATU_KBLOCK, see
+// xatu_kstored): there the mirror block is written only where it reaches that
+// triangle, next to the diagonal.
 //
 // Precision: T = double writes the complex128 matrix (parity mode).  T = float
 // writes the mixed-precision form used by the tensor-core solver: the band
 // energies scissor + E_c - E_v as an FP64 diagonal, and the interaction
-// kernel K = H - diag in two BF16 planes, K ~= K_hi + K_lo.#pragma once
+// kernel K = H - diag in two BF16 planes, K ~= K_hi + K_lo.
+#pragma once
 #include "params.h"
-
-
 
 __device__ __forceinline__ void split_store(__nv_bfloat162* hi, __nv_bfloat162* lo, int64_t idx, float re, float im) {
   const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
@@ -374,8 +376,9 @@ __device__ __forceinline__ void assemble_tile(const AsmParams& p, const AsmInput
         }
       }
     }
-    if (kb != kb2) {
-      // mirror block: rows col0 + c, columns row0 + r, conjugate transpose
+    // mirror block (rows col0 + c, columns row0 + r, conjugate transpose): only where it reaches the stored
+    // upper block triangle of the kernel planes (xatu_kstored), i.e. near the diagonal
+    if (kb != kb2 && (row0 + rows - 1) / XATU_KBLOCK >= col0 / XATU_KBLOCK) {
       constexpr int RV = (TR + VEC - 1) / VEC;
       for (int t = tid; t < TR * RV; t += blockDim.x) {
         const int c = t / RV, r = (t - c * RV) * VEC;

@@ -49,7 +49,7 @@
 #define BD_RR_THREADS HEEV_THREADS
 
 struct BDav {
-  long long N, ldk, ldb;
+  long long N, ldk, ldb, ldu;
   const __nv_bfloat162* Khi;
   const __nv_bfloat162* Klo;
   const double* diag;       // FP64 band-energy diagonal
@@ -69,9 +69,11 @@ struct BDav {
   cd* S;                    // BD_MAXB x BD_MAXB
   double* theta;            // BD_MMAX
   double* norms;            // BD_MAXB
-  float* Yf;                // N x 2 bp (tcgen05 output)
-  __nv_bfloat16* Bhi;       // 2 bp x ldb
+  float* Yf;                // N x 2 bp, row-major (tcgen05 output)
+  __nv_bfloat16* Bhi;       // 2 bp x ldb: operand along the interleaved columns of K
   __nv_bfloat16* Blo;
+  __nv_bfloat16* Uhi;       // 2 bp x ldu: operand along the rows of K
+  __nv_bfloat16* Ulo;
   int m, k, active, iters, stalled, kmask, restart;
 };
 
@@ -119,14 +121,22 @@ __global__ void __launch_bounds__(BD_ROWS) bd_build_bt_kernel(BDGlobal g, BDav* 
       re = (float)v.x;
       im = (float)v.y;
     }
-    const float vals[4] = {re, -im, im, re};
-    const long long o[4] = {(long long)s * d.ldb + 2 * j, (long long)s * d.ldb + 2 * j + 1,
-                            (long long)(g.bp + s) * d.ldb + 2 * j, (long long)(g.bp + s) * d.ldb + 2 * j + 1};
+    // the operand layouts of the tcgen05 product (hx_tc.cu): Bt along the interleaved columns, Bu along rows
+    const float vals[6] = {re, -im, im, re, re, im};
+    const long long o[6] = {(long long)s * d.ldb + 2 * j, (long long)s * d.ldb + 2 * j + 1,
+                            (long long)(g.bp + s) * d.ldb + 2 * j, (long long)(g.bp + s) * d.ldb + 2 * j + 1,
+                            (long long)s * d.ldu + j, (long long)(g.bp + s) * d.ldu + j};
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < 6; q++) {
       const __nv_bfloat16 h = __float2bfloat16_rn(vals[q]);
-      d.Bhi[o[q]] = h;
-      d.Blo[o[q]] = __float2bfloat16_rn(vals[q] - __bfloat162float(h));
+      const __nv_bfloat16 l = __float2bfloat16_rn(vals[q] - __bfloat162float(h));
+      if (q < 4) {
+        d.Bhi[o[q]] = h;
+        d.Blo[o[q]] = l;
+      } else {
+        d.Uhi[o[q]] = h;
+        d.Ulo[o[q]] = l;
+      }
     }
   }
 }
@@ -141,7 +151,8 @@ __global__ void __launch_bounds__(BD_ROWS) bd_finish_append_kernel(BDGlobal g, B
   const double di = d.diag[i];
   for (int s = 0; s < d.k; s++) {
     const cd p = d.P[(long long)s * d.N + i];
-    const cd w = mk((double)d.Yf[(long long)s * d.N + i] + di * p.x, (double)d.Yf[(long long)(g.bp + s) * d.N + i] + di * p.y);
+    const float* y = d.Yf + i * 2 * g.bp;
+    const cd w = mk((double)y[s] + di * p.x, (double)y[g.bp + s] + di * p.y);
     d.V[(long long)(d.m + s) * d.N + i] = p;
     d.W[(long long)(d.m + s) * d.N + i] = w;
   }
@@ -728,8 +739,8 @@ static xatu_status enqueue_iteration(xatu_batch* b) {
   for (size_t i = 0; i < b->members.size(); i++) {
     const BDav& h = b->hdesc[i];
     const int ng = 2 * g.bp;
-    BCK(xatu_launch_hx_tc(h.Khi, h.Klo, h.N, h.ldk, h.Bhi, h.Blo, h.ldb, ng, h.Yf, status, b->num_sms, b->stream,
-                          &D[i].active));
+    BCK(xatu_launch_hx_tc(h.Khi, h.Klo, h.N, h.ldk, h.Bhi, h.Blo, h.ldb, h.Uhi, h.Ulo, h.ldu, ng, h.Yf, status,
+                          b->num_sms, b->stream, &D[i].active));
   }
   bd_finish_append_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_prep_kernel<<<g.nmem, 256, 0, b->stream>>>(g, D);
@@ -865,13 +876,14 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   size_t total = 0;
   for (int i = 0; i < nmem; i++) {
     const long long N = b->members[i]->N;
-    const long long ldb = (2 * N + 7) / 8 * 8;
+    const long long ldb = (2 * N + 7) / 8 * 8, ldu = (N + 7) / 8 * 8;
     offs[i] = total;
     total += al(N * sizeof(double)) + 2 * al((size_t)N * mmax * sizeof(cd)) + 3 * al((size_t)N * BD_MAXB * sizeof(cd)) +
              3 * al((size_t)BD_MMAX * BD_MMAX * sizeof(cd)) + 2 * al((size_t)BD_MMAX * BD_MAXB * sizeof(cd)) +
              3 * al((size_t)BD_MAXB * BD_MAXB * sizeof(cd)) + al(BD_MMAX * sizeof(double)) +
              al(BD_MAXB * sizeof(double)) + al((size_t)N * 2 * b->g.bp * sizeof(float)) +
-             2 * al((size_t)2 * b->g.bp * ldb * sizeof(__nv_bfloat16));
+             2 * al((size_t)2 * b->g.bp * ldb * sizeof(__nv_bfloat16)) +
+             2 * al((size_t)2 * b->g.bp * ldu * sizeof(__nv_bfloat16));
   }
   BCK(b->d_arena.ensure(total));
   BCK(cudaMemsetAsync(b->d_arena.p, 0, total, b->stream));
@@ -889,6 +901,7 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     d.N = N;
     d.ldk = ctx->ldk;
     d.ldb = (2 * N + 7) / 8 * 8;
+    d.ldu = (N + 7) / 8 * 8;
     d.Khi = ctx->d_Khi.as<__nv_bfloat162>();
     d.Klo = ctx->d_Klo.as<__nv_bfloat162>();
     d.diag = ctx->d_diag.as<double>();
@@ -911,6 +924,8 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     d.Yf = reinterpret_cast<float*>(take((size_t)N * 2 * b->g.bp * sizeof(float)));
     d.Bhi = reinterpret_cast<__nv_bfloat16*>(take((size_t)2 * b->g.bp * d.ldb * sizeof(__nv_bfloat16)));
     d.Blo = reinterpret_cast<__nv_bfloat16*>(take((size_t)2 * b->g.bp * d.ldb * sizeof(__nv_bfloat16)));
+    d.Uhi = reinterpret_cast<__nv_bfloat16*>(take((size_t)2 * b->g.bp * d.ldu * sizeof(__nv_bfloat16)));
+    d.Ulo = reinterpret_cast<__nv_bfloat16*>(take((size_t)2 * b->g.bp * d.ldu * sizeof(__nv_bfloat16)));
   }
   BCK(b->d_desc.ensure(nmem * sizeof(BDav)));
   BCK(cudaMemcpyAsync(b->d_desc.p, b->hdesc.data(), nmem * sizeof(BDav), cudaMemcpyHostToDevice, b->stream));

@@ -241,6 +241,16 @@ __device__ __forceinline__ int equivalent_index(const EquivMap& m, double dx, do
   return (int)acc;
 }
 
+// ----------------------------------------------------------------- Hermitian block storage of the mixed kernel
+// The split-BF16 interaction kernel K of a mixed build keeps only its upper block triangle: with blocks of
+// XATU_KBLOCK x XATU_KBLOCK elements, block (I, J) is stored for J >= I (the diagonal blocks in full); the
+// rest of the N x ldk planes is never written or read.  K_rc for any (r, c) is K[r][c] where stored, else
+// conj(K[c][r]).
+#define XATU_KBLOCK 128
+__host__ __device__ __forceinline__ bool xatu_kstored(long long r, long long c) {
+  return (c / XATU_KBLOCK) >= (r / XATU_KBLOCK);
+}
+
 // ----------------------------------------------------------------- error flag
 // Kernels never trap: out-of-contract indices are recorded in a device word the
 // host reads after the stage.

@@ -45,12 +45,25 @@ __global__ void dav_diag_fp64_kernel(const cd* __restrict__ H, long long N, doub
 }
 
 // V[:, col0 + s] = e_{idx[s]}
-__global__ void dav_unit_vectors_kernel(cd* V, long long N, int col0, const int* idx, int nvec) {
+// Start block: column s = e_idx[s] + noise * xi_s, xi_s a fixed pseudo-random vector (splitmix64 of (i, s),
+// entries uniform in [-1, 1)).  The reference starts from unit vectors (davidson.cpp:16).  Unit vectors alone can leave a symmetry sector of H without a start vector
+// for every copy of a degenerate level (spin-degenerate models: H is block diagonal, the unit vectors of
+// the lowest diagonal entries fall unevenly in the blocks), and no correction ever leaves its block; the
+// noise gives every column a component in every sector.
+__device__ __forceinline__ double dav_noise(unsigned long long i, unsigned long long s) {
+  unsigned long long z = i * 0x9E3779B97F4A7C15ull + (s + 1) * 0xD1B54A32D192ED03ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+__global__ void dav_start_vectors_kernel(cd* V, long long N, int col0, const int* idx, int nvec, double noise) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= N * nvec) return;
   const int s = (int)(t / N);
   const long long i = t - (long long)s * N;
-  V[(long long)(col0 + s) * N + i] = mk(i == idx[s] ? 1.0 : 0.0, 0.0);
+  V[(long long)(col0 + s) * N + i] = mk((i == idx[s] ? 1.0 : 0.0) + noise * dav_noise(i, s), 0.0);
 }
 
 // X (row-major N x nv, complex float) <- V[:, col0 : col0 + nv]
@@ -147,30 +160,7 @@ dav_heev_kernel(const cd* __restrict__ T, int ldt, int m, int k, double* __restr
 // Bt operand of the tensor-core product (hx_tc.cu) from V[:, col0 : col0 + b]:
 //   rows [0, bp):   Re X at 2j, -Im X at 2j+1;   rows [bp, 2bp): Im X at 2j, Re X at 2j+1
 // (bp = b rounded up to 8; padding rows are zero), split into BF16 hi + lo.
-__global__ void dav_build_bt_kernel(const cd* __restrict__ V, long long N, int col0, int b, int bp, long long ldb,
-                                    __nv_bfloat16* __restrict__ Bhi, __nv_bfloat16* __restrict__ Blo) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= N * bp) return;
-  const int s = (int)(t / N);
-  const long long j = t - (long long)s * N;
-  float re = 0.f, im = 0.f;
-  if (s < b) {
-    const cd v = V[(long long)(col0 + s) * N + j];
-    re = (float)v.x;
-    im = (float)v.y;
-  }
-  const float vals[4] = {re, -im, im, re};
-  const long long off[4] = {(long long)s * ldb + 2 * j, (long long)s * ldb + 2 * j + 1,
-                            (long long)(bp + s) * ldb + 2 * j, (long long)(bp + s) * ldb + 2 * j + 1};
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const __nv_bfloat16 h = __float2bfloat16_rn(vals[q]);
-    Bhi[off[q]] = h;
-    Blo[off[q]] = __float2bfloat16_rn(vals[q] - __bfloat162float(h));
-  }
-}
-
-// W[:, col0 + s] = (Y_re[:, s], Y_im[:, s]) + d .* V[:, col0 + s]; Y column-major N x 2bp.
+// W[:, col0 + s] = (Y[:, s], Y[:, bp + s]) + d .* V[:, col0 + s]; Y row-major N x 2bp.
 __global__ void dav_finish_w_tc_kernel(const float* __restrict__ Y, const double* __restrict__ d,
                                        const cd* __restrict__ V, long long N, int col0, int b, int bp,
                                        cd* __restrict__ W) {
@@ -180,7 +170,8 @@ __global__ void dav_finish_w_tc_kernel(const float* __restrict__ Y, const double
   const long long i = t - (long long)s * N;
   const long long o = (long long)(col0 + s) * N + i;
   const cd v = V[o];
-  W[o] = mk((double)Y[(long long)s * N + i] + d[i] * v.x, (double)Y[(long long)(bp + s) * N + i] + d[i] * v.y);
+  const float* y = Y + i * 2 * bp;
+  W[o] = mk((double)y[s] + d[i] * v.x, (double)y[bp + s] + d[i] * v.y);
 }
 
 static bool tc_usable(const xatu_ctx* ctx) {
@@ -202,23 +193,25 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
     return XATU_OK;
   }
   if (tc_usable(ctx)) {
-    const long long ldb = (2 * N + 7) / 8 * 8;
-    for (int c = 0; c < nv; c += 32) {
-      const int b = std::min(32, nv - c);
+    const long long ldb = (2 * N + 7) / 8 * 8, ldu = (N + 7) / 8 * 8;
+    constexpr int MAXB = XATU_HX_TC_MAXB;
+    for (int c = 0; c < nv; c += MAXB) {
+      const int b = std::min(MAXB, nv - c);
       const int bp = (b + 7) / 8 * 8;
       const int ng = 2 * bp;
-      XATU_CK(ctx->dv_Bop.ensure((size_t)64 * ldb * sizeof(__nv_bfloat16)));
-      XATU_CK(ctx->dv_Blo.ensure((size_t)64 * ldb * sizeof(__nv_bfloat16)));
-      XATU_CK(ctx->dv_Yf.ensure((size_t)N * 64 * sizeof(float)));
-      const long long tb = N * bp;
-      dav_build_bt_kernel<<<(int)((tb + threads - 1) / threads), threads, 0, ctx->stream>>>(
-          V, N, col0 + c, b, bp, ldb, ctx->dv_Bop.as<__nv_bfloat16>(), ctx->dv_Blo.as<__nv_bfloat16>());
+      XATU_CK(ctx->dv_Bop.ensure((size_t)2 * MAXB * ldb * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Blo.ensure((size_t)2 * MAXB * ldb * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Uhi.ensure((size_t)2 * MAXB * ldu * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Ulo.ensure((size_t)2 * MAXB * ldu * sizeof(__nv_bfloat16)));
+      XATU_CK(ctx->dv_Yf.ensure((size_t)N * 2 * MAXB * sizeof(float)));
+      XATU_CK(xatu_launch_hx_operands(V + (long long)(col0 + c) * N, N, N, b, bp, ctx->dv_Bop.p, ctx->dv_Blo.p, ldb,
+                                      ctx->dv_Uhi.p, ctx->dv_Ulo.p, ldu, ctx->stream));
       ctx->launches++;
-      XATU_CK(cudaGetLastError());
       if (c == 0) XATU_CK(cudaEventRecord(ctx->ev[8], ctx->stream));
-      XATU_CK(xatu_launch_hx_tc(ctx->d_Khi.p, ctx->d_Klo.p, N, ctx->ldk, ctx->dv_Bop.p, ctx->dv_Blo.p, ldb, ng,
-                                ctx->dv_Yf.as<float>(), ctx->d_status.as<int>(), ctx->num_sms, ctx->stream));
-      if (c + 32 >= nv) XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
+      XATU_CK(xatu_launch_hx_tc(ctx->d_Khi.p, ctx->d_Klo.p, N, ctx->ldk, ctx->dv_Bop.p, ctx->dv_Blo.p, ldb,
+                                ctx->dv_Uhi.p, ctx->dv_Ulo.p, ldu, ng, ctx->dv_Yf.as<float>(), ctx->d_status.as<int>(),
+                                ctx->num_sms, ctx->stream));
+      if (c + MAXB >= nv) XATU_CK(cudaEventRecord(ctx->ev[9], ctx->stream));
       ctx->hx_pending = true;
       ctx->hx_calls++;
       ctx->hx_last_path = 2;
@@ -410,8 +403,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
   XATU_CK(cudaMemcpyAsync(sel_dev, order.data(), bsz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   XATU_CK(cudaMemcpyAsync(dkept, &bsz, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   {
+    // unit vectors of the lowest diagonal entries plus noise of norm ~1e-3 per column, orthonormalised below
+    // (enough to seed every symmetry sector; larger noise costs Davidson steps to remove again)
     const long long tot = N * bsz;
-    dav_unit_vectors_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(V, N, 0, sel_dev, bsz);
+    const double noise = N > bsz ? 1e-3 * std::sqrt(3.0 / (double)N) : 0.0;
+    dav_start_vectors_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(V, N, 0, sel_dev, bsz,
+                                                                                                noise);
     ctx->launches++;
     XATU_CK(cudaGetLastError());
   }
@@ -423,6 +420,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(xatu_raise_smem_limit((const void*)ts_ritz_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_gram_orth_kernel, ts_gram_orth_smem(DAV_MAX_BASIS - bmax, bmax)));
   }
+  if (N > bsz) XATU_TRY(orthonormalize_block(ctx, N, 0, bsz));
 
   // Thick-restart block Davidson on the basis V (W = H V):
   //   T[:, new] = V^H W[:, new] (the old block of T is kept);  lowest nritz Ritz pairs of T;

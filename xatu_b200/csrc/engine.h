@@ -96,7 +96,7 @@ struct xatu_ctx {
   int num_sms = 148;
   int dav_iters = 0;
   double dav_maxres = 0;
-  DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo;
+  DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo, dv_Uhi, dv_Ulo;
   DBuf dv_part;                // per-tile partial sums of the Davidson reductions
   void* h_small = nullptr;     // pinned host staging for small read-backs (4 KB)
 
@@ -163,12 +163,20 @@ xatu_status xatu_adjoint_weighted(xatu_ctx* ctx, const cd* Y, const cd* Zc, cons
 // K.X products (hx.cu).  Y[N x b] = (Khi + Klo) X, all row-major complex float.
 cudaError_t xatu_launch_hx_cuda_core(const __nv_bfloat162* Khi, const __nv_bfloat162* Klo, long long ldk, const float2* X,
                                      float2* Y, long long N, int b, cudaStream_t s);
-// tcgen05 version (hx_tc.cu): Bt operands (ng x ldb bf16, hi/lo), Y column-major N x ng FP32.
+// tcgen05 version (hx_tc.cu) over the upper block triangle of K: operands Bt (ng x ldb bf16, hi/lo) and
+// Bu (ng x ldu bf16, hi/lo) from xatu_launch_hx_operands, ng in {16, 32, 48}; Y row-major N x ng FP32
+// (columns s < ng/2 the real parts, ng/2 + s the imaginary parts), zeroed here.
 // active: NULL, or a device word read by the kernel; 0 skips the product (Y is still zeroed).
 cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, long long ldk, const void* Bhi,
-                              const void* Blo, long long ldb, int ng, float* Y, int* status, int num_sms,
-                              cudaStream_t s, const int* active = nullptr);
+                              const void* Blo, long long ldb, const void* Uhi, const void* Ulo, long long ldu, int ng,
+                              float* Y, int* status, int num_sms, cudaStream_t s, const int* active = nullptr);
+// Operand planes of the tcgen05 product from b columns of X (complex FP64, column stride ldx), padded to bp:
+// ldb >= 2N and ldu >= N, both multiples of 8.
+cudaError_t xatu_launch_hx_operands(const cd* X, long long ldx, long long N, int b, int bp, void* Bhi, void* Blo,
+                                    long long ldb, void* Uhi, void* Ulo, long long ldu, cudaStream_t s);
 size_t xatu_hx_tc_smem(int ng);
+// Widest block of vectors one tcgen05 product takes (ng = 2 * 24 = 48).
+#define XATU_HX_TC_MAXB 24
 // W[:, col0 : col0 + nv] = H V[:, col0 : col0 + nv] with the current build (davidson.cu).
 xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv);
 // Adds the bracketed K.X device time of the last xatu_apply_h to hx_ms (call after a stream synchronisation).

@@ -1,8 +1,9 @@
 // Y = K X for the mixed-precision kernel K = K_hi + K_lo (two BF16 planes,
-// complex, row-major N x N) and a block X of b complex FP32 vectors
-// (row-major N x b).  CUDA-core version: 64-row x 32-column tiles of K are
-// combined (hi + lo) into FP32 in shared memory and reused by every vector of
-// the block; FP32 accumulation.
+// complex, row-major N x ldk, upper block triangle stored: xatu_kstored) and a
+// block X of b complex FP32 vectors (row-major N x b).  CUDA-core version:
+// 64-row x 32-column tiles of K are combined (hi + lo) into FP32 in shared
+// memory and reused by every vector of the block; elements below the stored
+// block triangle are read as the conjugate of their mirror; FP32 accumulation.
 #include "engine.h"
 
 #define HX_ROWS 64
@@ -29,9 +30,12 @@ hx_cuda_core_kernel(const __nv_bfloat162* __restrict__ Khi, const __nv_bfloat162
       const long long gr = row0 + rr, gc = c0 + cc;
       float2 v = make_float2(0.f, 0.f);
       if (gr < N && gc < N) {
-        const __nv_bfloat162 h = Khi[gr * ldk + gc], l = Klo[gr * ldk + gc];
+        const bool st = xatu_kstored(gr, gc);
+        const long long o = st ? gr * ldk + gc : gc * ldk + gr;
+        const __nv_bfloat162 h = Khi[o], l = Klo[o];
         v.x = __bfloat162float(h.x) + __bfloat162float(l.x);
         v.y = __bfloat162float(h.y) + __bfloat162float(l.y);
+        if (!st) v.y = -v.y;
       }
       sK[rr][cc] = v;
     }

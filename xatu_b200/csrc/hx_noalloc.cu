@@ -13,8 +13,10 @@
 // mixed build, and x) and the output y, all in device memory.  The scratch the
 // tensor-core product needs -- the BF16 operand planes built from x, the FP32
 // accumulator and a status word -- lives in one file-scope __device__ array of
-// fixed size (6 MB + 256 B), which every GPU that loads this library holds
+// fixed size (8 MB + 256 B), which every GPU that loads this library holds
 // until the process exits.
+#include <cuda.h>
+
 #include <cstdio>
 #include <mutex>
 
@@ -26,11 +28,14 @@
 
 namespace {
 
-constexpr long long kMaxLdb = 2LL * XATU_NOALLOC_MAX_N;          // bf16 per operand row (multiple of 8)
+constexpr long long kMaxLdb = 2LL * XATU_NOALLOC_MAX_N;          // bf16 per Bt operand row (multiple of 8)
+constexpr long long kMaxLdu = XATU_NOALLOC_MAX_N;                // bf16 per Bu operand row (multiple of 8)
 constexpr int kMaxRows = 2 * XATU_NOALLOC_MAX_NVEC;             // operand rows: Re block + Im block
-constexpr size_t kPlaneBytes = (size_t)kMaxRows * kMaxLdb * 2;  // 2 MB per BF16 plane
+constexpr size_t kPlaneBytes = (size_t)kMaxRows * kMaxLdb * 2;  // 2 MB per Bt plane
+constexpr size_t kUPlaneBytes = (size_t)kMaxRows * kMaxLdu * 2; // 1 MB per Bu plane
 constexpr size_t kAccBytes = (size_t)XATU_NOALLOC_MAX_N * kMaxRows * sizeof(float);  // 2 MB
-constexpr size_t kScratchBytes = 2 * kPlaneBytes + kAccBytes + 256;
+constexpr size_t kScratchBytes = 2 * kPlaneBytes + 2 * kUPlaneBytes + kAccBytes + 256;
+static_assert(XATU_NOALLOC_MAX_NVEC <= XATU_HX_TC_MAXB, "one tensor-core product per call");
 
 }  // namespace
 
@@ -40,18 +45,42 @@ static __device__ __align__(256) unsigned char g_hx_noalloc_scratch[kScratchByte
 
 namespace {
 
+// The driver's handle of the current context, looked up through the runtime's entry-point table so that the
+// library does not link libcuda directly.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  }
+  return fn;
+}
+
 std::mutex g_setup_mu;
 void* g_scratch_addr[64] = {};
+CUcontext g_scratch_ctx[64] = {};
 int g_num_sms[64] = {};
 
-// Once per device, with that device current: the device address of the scratch.
+// Once per device and context, with that device current: the device address of the scratch.  The address
+// is looked up again when the device's context changed since the last call (after cudaDeviceReset or a
+// released and recreated primary context, the module and its array are loaded anew).
 xatu_status noalloc_setup(int dev, unsigned char** base, int* sms) {
   std::lock_guard<std::mutex> lock(g_setup_mu);
   if (dev < 0 || dev >= 64) {
     fprintf(stderr, "xatu_hx_noalloc: device ordinal %d out of range\n", dev);
     return XATU_ERR_UNSUPPORTED;
   }
-  if (!g_scratch_addr[dev]) {
+  CUcontext cur = nullptr;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (!get || get(&cur) != CUDA_SUCCESS) {
+    fprintf(stderr, "xatu_hx_noalloc: cannot query the current CUDA context\n");
+    return XATU_ERR_CUDA;
+  }
+  if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != cur) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_hx_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) {
@@ -60,7 +89,9 @@ xatu_status noalloc_setup(int dev, unsigned char** base, int* sms) {
     }
     int n = 0;
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    if (get(&cur) != CUDA_SUCCESS) return XATU_ERR_CUDA;   // the lookup may have created the primary context
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = cur;
     g_num_sms[dev] = n;
   }
   *base = static_cast<unsigned char*>(g_scratch_addr[dev]);
@@ -70,33 +101,7 @@ xatu_status noalloc_setup(int dev, unsigned char** base, int* sms) {
 
 }  // namespace
 
-// Operand planes from x (column-major n x nvec complex): row s (< bp) holds
-// (Re x_js, -Im x_js) at columns (2j, 2j+1), row bp + s holds (Im x_js, Re x_js);
-// rows of padding vectors are zero.  BF16 hi + lo split.
-__global__ void hx_noalloc_operand_kernel(const cd* __restrict__ x, long long n, int nvec, int bp, long long ldb,
-                                          __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= n * bp) return;
-  const int s = (int)(t / n);
-  const long long j = t - (long long)s * n;
-  float re = 0.f, im = 0.f;
-  if (s < nvec) {
-    const cd v = x[(long long)s * n + j];
-    re = (float)v.x;
-    im = (float)v.y;
-  }
-  const float vals[4] = {re, -im, im, re};
-  const long long off[4] = {(long long)s * ldb + 2 * j, (long long)s * ldb + 2 * j + 1,
-                            (long long)(bp + s) * ldb + 2 * j, (long long)(bp + s) * ldb + 2 * j + 1};
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const __nv_bfloat16 h = __float2bfloat16_rn(vals[q]);
-    hi[off[q]] = h;
-    lo[off[q]] = __float2bfloat16_rn(vals[q] - __bfloat162float(h));
-  }
-}
-
-// y[:, s] = acc (Re rows s, Im rows bp + s) + diag .* x[:, s], in FP64.
+// y[:, s] = acc (row i: Re in column s, Im in column bp + s) + diag .* x[:, s], in FP64.
 __global__ void hx_noalloc_finish_kernel(const float* __restrict__ acc, const double* __restrict__ diag,
                                          const cd* __restrict__ x, long long n, int nvec, int bp, cd* __restrict__ y) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -104,7 +109,8 @@ __global__ void hx_noalloc_finish_kernel(const float* __restrict__ acc, const do
   const int s = (int)(t / n);
   const long long i = t - (long long)s * n;
   const cd v = x[t];
-  y[t] = mk((double)acc[(long long)s * n + i] + diag[i] * v.x, (double)acc[(long long)(bp + s) * n + i] + diag[i] * v.y);
+  const float* a = acc + i * 2 * bp;
+  y[t] = mk((double)a[s] + diag[i] * v.x, (double)a[bp + s] + diag[i] * v.y);
 }
 
 extern "C" xatu_status xatu_hx_noalloc(const void* k_hi, const void* k_lo, const double* diag, int64_t n, int64_t ldk,
@@ -132,6 +138,17 @@ extern "C" xatu_status xatu_hx_noalloc(const void* k_hi, const void* k_lo, const
     fprintf(stderr, "xatu_hx_noalloc: device pointers must be 16-byte aligned\n");
     return XATU_ERR_INVALID;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  {
+    // the call reads its status word back and waits for the stream, which a stream capture does not allow
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) return XATU_ERR_CUDA;
+    if (cs != cudaStreamCaptureStatusNone) {
+      fprintf(stderr, "xatu_hx_noalloc: the stream is being captured; the call waits for its stream and cannot "
+                      "run inside a capture\n");
+      return XATU_ERR_STATE;
+    }
+  }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return XATU_ERR_CUDA;
   unsigned char* base = nullptr;
@@ -140,22 +157,24 @@ extern "C" xatu_status xatu_hx_noalloc(const void* k_hi, const void* k_lo, const
   if (st != XATU_OK) return st;
   __nv_bfloat16* op_hi = reinterpret_cast<__nv_bfloat16*>(base);
   __nv_bfloat16* op_lo = reinterpret_cast<__nv_bfloat16*>(base + kPlaneBytes);
-  float* acc = reinterpret_cast<float*>(base + 2 * kPlaneBytes);
-  int* status = reinterpret_cast<int*>(base + 2 * kPlaneBytes + kAccBytes);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  __nv_bfloat16* ou_hi = reinterpret_cast<__nv_bfloat16*>(base + 2 * kPlaneBytes);
+  __nv_bfloat16* ou_lo = reinterpret_cast<__nv_bfloat16*>(base + 2 * kPlaneBytes + kUPlaneBytes);
+  float* acc = reinterpret_cast<float*>(base + 2 * kPlaneBytes + 2 * kUPlaneBytes);
+  int* status = reinterpret_cast<int*>(base + 2 * kPlaneBytes + 2 * kUPlaneBytes + kAccBytes);
   const int bp = (nvec + 7) / 8 * 8;
   const int ng = 2 * bp;
-  const long long ldb = (2 * n + 7) / 8 * 8;
+  const long long ldb = (2 * n + 7) / 8 * 8, ldu = (n + 7) / 8 * 8;
   // the status word keeps the last call's value: clear it
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), s);
   if (e != cudaSuccess) goto cuda_error;
   {
-    const long long t1 = n * bp;
-    hx_noalloc_operand_kernel<<<(unsigned)((t1 + 255) / 256), 256, 0, s>>>(reinterpret_cast<const cd*>(x), n, nvec,
-                                                                           bp, ldb, op_hi, op_lo);
-    if ((e = cudaGetLastError()) != cudaSuccess) goto cuda_error;
+    // every operand row (padding rows included) is rewritten from x: nothing of an earlier call is read
+    if ((e = xatu_launch_hx_operands(reinterpret_cast<const cd*>(x), n, n, nvec, bp, op_hi, op_lo, ldb, ou_hi, ou_lo,
+                                     ldu, s)) != cudaSuccess)
+      goto cuda_error;
     // the product zeroes the accumulator before it adds into it
-    if ((e = xatu_launch_hx_tc(k_hi, k_lo, n, ldk, op_hi, op_lo, ldb, ng, acc, status, sms, s)) != cudaSuccess)
+    if ((e = xatu_launch_hx_tc(k_hi, k_lo, n, ldk, op_hi, op_lo, ldb, ou_hi, ou_lo, ldu, ng, acc, status, sms, s)) !=
+        cudaSuccess)
       goto cuda_error;
     const long long t2 = n * nvec;
     hx_noalloc_finish_kernel<<<(unsigned)((t2 + 255) / 256), 256, 0, s>>>(acc, diag, reinterpret_cast<const cd*>(x), n,
@@ -164,6 +183,12 @@ extern "C" xatu_status xatu_hx_noalloc(const void* k_hi, const void* k_lo, const
     int h_status = 0;
     if ((e = cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess) goto cuda_error;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) goto cuda_error;
+    if (h_status & XATU_DEVERR_INDEX) {
+      // a CTA's row range spans more accumulators than the kernel holds: a launch-geometry fault of the library
+      fprintf(stderr, "xatu_hx_noalloc: internal error, tile range outside the kernel's accumulators (status %d)\n",
+              h_status);
+      return XATU_ERR_INVALID;
+    }
     if (h_status != 0) {
       fprintf(stderr, "xatu_hx_noalloc: a tensor-core pipeline wait timed out (status %d)\n", h_status);
       return XATU_ERR_NOT_CONVERGED;

@@ -63,7 +63,7 @@ struct AsmInputs {
 
 struct AsmOutputs {
   cd* H;                   // FP64: N x N
-  __nv_bfloat162* Khi;     // MIXED: N x N
+  __nv_bfloat162* Khi;     // MIXED: N x ldk, upper block triangle (xatu_kstored)
   __nv_bfloat162* Klo;
   double* diag;            // MIXED: N
 };
