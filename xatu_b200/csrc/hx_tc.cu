@@ -24,22 +24,26 @@
 // by row block, are cut into equal contiguous ranges, one per CTA.
 //   * warp 0: TMA producer, an XHH_STAGES-deep ring of stages (A_hi, A_lo, Bt_hi, Bt_lo, Bu_hi, Bu_lo);
 //   * warp 1: one thread issues tcgen05.mma (M = 128, N = ng, K = 16).  The direct accumulator of a row block
-//     (a segment of the range) and the transposed accumulator of a tile each take a slot of a ring of two in
-//     tensor memory; tcgen05.commit frees ring stages and publishes finished accumulators;
+//     (a segment of the range) takes a slot of a ring of two in tensor memory, the transposed accumulator of a
+//     tile one of a ring of XHH_TSLOTS; tcgen05.commit frees ring stages and publishes finished accumulators;
 //   * warps 4-7: epilogue, tcgen05.ld of the accumulator lanes, FP32 vector atomics into Y (row-major N x ng),
 //     then an arrive that frees the accumulator slot;
 //   * every wait is bounded; on timeout the CTA records an error word, drains its tensor-core work (bounded)
 //     and frees its tensor memory.
+// The host caches the six tensor maps of recent launches (a Davidson solve repeats the same product).
 #include <cuda.h>
 #include <cudaTypedefs.h>
+
+#include <mutex>
 
 #include "engine.h"
 
 #define XHH_BM 128            // rows of a tile (one row block)
 #define XHH_BOX 64            // bf16 per TMA box row: 128 bytes, the swizzle width
 #define XHH_STAGES 2
+#define XHH_TSLOTS 4          // transposed accumulators in tensor memory (the epilogue drains while the MMA runs on)
 #define XHH_THREADS 256
-#define XHH_TMEM_COLS 256
+#define XHH_TMEM_COLS 512     // 2 direct + XHH_TSLOTS transposed slots of ng <= 48 columns
 #define XHH_SPIN_LIMIT (1u << 26)
 
 static_assert(XATU_KBLOCK == 2 * 64 && XHH_BM == XATU_KBLOCK, "tile geometry assumes 128-blocks of 64-column tiles");
@@ -166,7 +170,7 @@ struct HxTcSmem {
   uint64_t full[XHH_STAGES];
   uint64_t empty[XHH_STAGES];
   uint64_t dfull[2], dempty[2];   // direct accumulator slots
-  uint64_t tfull[2], tempty[2];   // transposed accumulator slots
+  uint64_t tfull[XHH_TSLOTS], tempty[XHH_TSLOTS];   // transposed accumulator slots
   uint64_t drain;
   uint32_t tmem_base;
   int abort_flag;
@@ -206,6 +210,8 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
     for (int a = 0; a < 2; a++) {
       mbar_init(&sh->dfull[a], 1);
       mbar_init(&sh->dempty[a], 4);
+    }
+    for (int a = 0; a < XHH_TSLOTS; a++) {
       mbar_init(&sh->tfull[a], 1);
       mbar_init(&sh->tempty[a], 4);
     }
@@ -310,8 +316,9 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
         }
         dfresh = false;
         if (!diag) {
-          const uint32_t tslot = (uint32_t)(tcount & 1);
-          if (tcount >= 2 && !mbar_wait(&sh->tempty[tslot], (uint32_t)(((tcount >> 1) - 1) & 1), abort_flag)) {
+          const uint32_t tslot = (uint32_t)(tcount % XHH_TSLOTS);
+          const int tuse = tcount / XHH_TSLOTS;
+          if (tuse >= 1 && !mbar_wait(&sh->tempty[tslot], (uint32_t)((tuse - 1) & 1), abort_flag)) {
             atomicOr(p.status, XATU_DEVERR_NOCONV);
             *abort_flag = 1;
             break;
@@ -353,8 +360,9 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
         curI = I;
       }
       if ((t >> 1) != I) {
-        const uint32_t tslot = (uint32_t)(tcount & 1);
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh->tfull[tslot], (uint32_t)((tcount >> 1) & 1), abort_flag));
+        const uint32_t tslot = (uint32_t)(tcount % XHH_TSLOTS);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&sh->tfull[tslot], (uint32_t)((tcount / XHH_TSLOTS) & 1),
+                                                          abort_flag));
         if (!ok) {
           if (lane == 0) atomicOr(p.status, XATU_DEVERR_NOCONV);
           *abort_flag = 1;
@@ -512,17 +520,63 @@ static cudaError_t launch_ng(const CUtensorMap* m, const HxTcParams& p, float* Y
   return cudaGetLastError();
 }
 
+namespace {
+// Tensor maps of recent launches: encoding six maps costs host time that a Davidson step would otherwise
+// wait for between its kernels.  Keyed by every argument the maps depend on.
+struct MapKey {
+  const void* ptr[6];
+  long long N, ldk, ldb, ldu;
+  int ng, dev;
+  bool operator==(const MapKey& o) const {
+    for (int i = 0; i < 6; i++)
+      if (ptr[i] != o.ptr[i]) return false;
+    return N == o.N && ldk == o.ldk && ldb == o.ldb && ldu == o.ldu && ng == o.ng && dev == o.dev;
+  }
+};
+struct MapEntry {
+  MapKey key;
+  CUtensorMap maps[6];
+  bool used = false;
+};
+std::mutex g_map_mu;
+MapEntry g_maps[16];
+int g_map_next = 0;
+}  // namespace
+
 cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, long long ldk, const void* Bhi,
                               const void* Blo, long long ldb, const void* Uhi, const void* Ulo, long long ldu, int ng,
                               float* Y, int* status, int num_sms, cudaStream_t s, const int* active) {
   if ((ng != 16 && ng != 32 && ng != 48) || (ldk % 4) != 0 || (ldb % 8) != 0 || (ldu % 8) != 0 || N < 1)
     return cudaErrorInvalidValue;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  MapKey key{{Khi, Klo, Bhi, Blo, Uhi, Ulo}, N, ldk, ldb, ldu, ng, dev};
   CUtensorMap m[6];
-  const uint64_t kdim = 2ull * N;
-  if (!make_map(&m[0], Khi, kdim, N, ldk * 4, XHH_BOX, XHH_BM) || !make_map(&m[1], Klo, kdim, N, ldk * 4, XHH_BOX, XHH_BM) ||
-      !make_map(&m[2], Bhi, kdim, ng, ldb * 2, XHH_BOX, ng) || !make_map(&m[3], Blo, kdim, ng, ldb * 2, XHH_BOX, ng) ||
-      !make_map(&m[4], Uhi, N, ng, ldu * 2, XHH_BOX, ng) || !make_map(&m[5], Ulo, N, ng, ldu * 2, XHH_BOX, ng))
-    return cudaErrorInvalidValue;
+  {
+    std::lock_guard<std::mutex> lock(g_map_mu);
+    int hit = -1;
+    for (int i = 0; i < 16; i++)
+      if (g_maps[i].used && g_maps[i].key == key) hit = i;
+    if (hit < 0) {
+      MapEntry& en = g_maps[g_map_next];
+      const uint64_t kdim = 2ull * N;
+      if (!make_map(&en.maps[0], Khi, kdim, N, ldk * 4, XHH_BOX, XHH_BM) ||
+          !make_map(&en.maps[1], Klo, kdim, N, ldk * 4, XHH_BOX, XHH_BM) ||
+          !make_map(&en.maps[2], Bhi, kdim, ng, ldb * 2, XHH_BOX, ng) ||
+          !make_map(&en.maps[3], Blo, kdim, ng, ldb * 2, XHH_BOX, ng) ||
+          !make_map(&en.maps[4], Uhi, N, ng, ldu * 2, XHH_BOX, ng) ||
+          !make_map(&en.maps[5], Ulo, N, ng, ldu * 2, XHH_BOX, ng)) {
+        en.used = false;
+        return cudaErrorInvalidValue;
+      }
+      en.key = key;
+      en.used = true;
+      hit = g_map_next;
+      g_map_next = (g_map_next + 1) % 16;
+    }
+    for (int i = 0; i < 6; i++) m[i] = g_maps[hit].maps[i];
+  }
   HxTcParams p;
   p.nb = (int)((N + XHH_BM - 1) / XHH_BM);
   p.nt = (int)((N + 63) / 64);
@@ -531,7 +585,7 @@ cudaError_t xatu_launch_hx_tc(const void* Khi, const void* Klo, long long N, lon
   p.status = status;
   p.active = active;
   const int grid = (int)std::min<long long>(num_sms, p.tiles);
-  cudaError_t e = cudaMemsetAsync(Y, 0, sizeof(float) * (size_t)N * ng, s);
+  e = cudaMemsetAsync(Y, 0, sizeof(float) * (size_t)N * ng, s);
   if (e != cudaSuccess) return e;
   if (ng == 16) return launch_ng<16>(m, p, Y, grid, s);
   if (ng == 32) return launch_ng<32>(m, p, Y, grid, s);
