@@ -140,7 +140,7 @@ def test_three_band_window_tiles(monkeypatch):
     ex, orc = _pair(cfg, 5, 3, [1., 4., 13.55], exchange=True)
     ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
     ex.BShamiltonian("fp64")
-    assert ex.kernelStats("assembly")[2] == 0          # tile path
+    assert ex.kernelStats("assembly")[2] == 0          # tile path (CUDA cores: FP64)
     H = ex.HBS
     assert rel_err(H, orc.bs_hamiltonian()) < FP64_TOL
     ex.BShamiltonian("mixed")
@@ -321,3 +321,27 @@ def test_reciprocal_exchange_16_states_vs_oracle():
     res = ex.diagonalize("davidson", 16)
     w = np.linalg.eigvalsh(orc.bs_hamiltonian())[:16]
     assert np.abs(res.eigval - w).max() < ENERGY_TOL
+
+
+@pytest.mark.parametrize("model,ncell,nbands,kw", [
+    ("MoS2.model", 10, 2, dict(Q=(0, 0.1, 0), exchange=True)),                 # 2v + 2c, tiles of 16 k points
+    ("MoS2.model", 5, 3, dict(exchange=True)),                                  # 3v + 3c, tiles of 8 k points
+    ("hBN.model", 14, 1, dict(mode="reciprocalspace", nG=3, exchange=True)),    # 1v + 1c, reciprocal space
+])
+def test_tensor_core_assembly(model, ncell, nbands, kw, monkeypatch):
+    """The mixed build with the band overlaps on tcgen05 (assembly path 2) against the oracle's FP64 matrix and
+    against the CUDA-core tile (path 0) on the same band stacks."""
+    cfg = model_config(model)
+    params = [1., 4., 13.55] if model == "MoS2.model" else [1, 1, 10]
+    ex, orc = _pair(cfg, ncell, nbands, params, **kw)
+    ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
+    ex.BShamiltonian("mixed")
+    assert ex.kernelStats("assembly")[2] == 2
+    H_tc = ex.HBS
+    Ho = orc.bs_hamiltonian()
+    assert rel_err(H_tc, Ho) < MIXED_TOL
+    assert np.array_equal(H_tc, H_tc.conj().T)
+    monkeypatch.setenv("XATU_ASSEMBLY_CUDA_CORE", "1")
+    ex.BShamiltonian("mixed")
+    assert ex.kernelStats("assembly")[2] == 0
+    assert rel_err(ex.HBS, H_tc) < MIXED_TOL

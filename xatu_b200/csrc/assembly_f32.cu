@@ -1,12 +1,41 @@
-// Single-system tile assembly, float: one CTA per upper-triangular (k-block, k'-block) tile
-// (assemble_tile, assembly_tile.cuh).  Tile side 16 k points for windows of up to 4 e-h pairs per k,
-// 8 for larger windows (the staging tile grows with (nv nc)^2).
-#include "assembly_tile.cuh"
+// Single-system tile assembly, float: one CTA per upper-triangular (k-block, k'-block) tile.  Tile side 16 k
+// points for windows of up to 4 e-h pairs per k, 8 for larger windows (the staging tile grows with (nv nc)^2).
+// The band overlaps run on the tensor cores (assemble_tile_tc, assembly_tc.cuh) when the orbital basis and
+// the window fit its products; otherwise, or with XATU_ASSEMBLY_CUDA_CORE=1 in the environment, on the CUDA
+// cores (assemble_tile, assembly_tile.cuh).
+#include <cstdlib>
+
+#include "assembly_tc.cuh"
 
 template <typename T, int NV, int NC, int NA, bool MIXED, int TK>
 __global__ void __launch_bounds__(TK * TK)
 bse_assemble_tile_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
   assemble_tile<T, NV, NC, NA, MIXED, TK>(p, in, out, nblk, blockIdx.x);
+}
+
+template <int NV, int NC, int NA, int TK>
+__global__ void __launch_bounds__(asm_tc_threads(TK))
+bse_assemble_tile_tc_kernel(AsmParams p, AsmInputs in, AsmOutputs out, int nblk) {
+  assemble_tile_tc<NV, NC, NA, TK>(p, in, out, nblk, blockIdx.x);
+}
+
+template <int NV, int NC, int NA>
+static cudaError_t launch_tile_tc(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s) {
+  constexpr int TK = (NV * NC <= 4) ? 16 : 8;
+  // one M = 128 product per overlap: atoms x k points x bands must fit its rows
+  if constexpr (NA * TK * NC > 128 || NA * TK * NV > 128 || 2 * TK * (NV + NC) > 256) {
+    return cudaErrorNotSupported;
+  } else {
+  const int nblk = (p.nk + TK - 1) / TK;
+  const int ntiles = nblk * (nblk + 1) / 2;
+  const AsmTcGeom g = asm_tc_geom<NV, NC, NA, TK>(p.norb);
+  if (g.KP > XATU_ASM_TC_KPMAX || g.bytes > 200 * 1024) return cudaErrorNotSupported;
+  auto kern = bse_assemble_tile_tc_kernel<NV, NC, NA, TK>;
+  cudaError_t e = xatu_raise_smem_limit((const void*)kern, g.bytes);
+  if (e != cudaSuccess) return e;
+  kern<<<ntiles, asm_tc_threads(TK), g.bytes, s>>>(p, in, out, nblk);
+  return cudaGetLastError();
+  }
 }
 
 template <typename T, int NV, int NC, int NA, bool MIXED>
@@ -28,14 +57,26 @@ static cudaError_t launch_tile(const AsmParams& p, const AsmInputs& in, const As
 
 // Launches the tile kernel of the band-window class of p; *launched = false when the class has none.
 cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
-                          bool* launched) {
+                          bool* launched, bool* tensor_cores) {
   *launched = true;
+  *tensor_cores = false;
+  const char* cc = std::getenv("XATU_ASSEMBLY_CUDA_CORE");
+  const bool allow_tc = !(cc && cc[0] == '1');
+  // the tensor-core tile first; cudaErrorNotSupported (orbital basis or staging too large) falls back
+#define XATU_TRY_TC(NVt, NCt, NAt)                                                           \
+  if (allow_tc) {                                                                            \
+    cudaError_t e = launch_tile_tc<NVt, NCt, NAt>(p, in, out, s);                             \
+    if (e != cudaErrorNotSupported) {                                                        \
+      *tensor_cores = e == cudaSuccess;                                                      \
+      return e;                                                                              \
+    }                                                                                        \
+  }
 #define XATU_CASE(NVv, NCv)                                                                  \
   if (p.nv == NVv && p.nc == NCv) {                                                          \
-    if (p.na == 1) return launch_tile<float, NVv, NCv, 1, true>(p, in, out, s);                 \
-    if (p.na == 2) return launch_tile<float, NVv, NCv, 2, true>(p, in, out, s);                 \
-    if (p.na == 3) return launch_tile<float, NVv, NCv, 3, true>(p, in, out, s);                 \
-    if (p.na == 4) return launch_tile<float, NVv, NCv, 4, true>(p, in, out, s);                 \
+    if (p.na == 1) { XATU_TRY_TC(NVv, NCv, 1) return launch_tile<float, NVv, NCv, 1, true>(p, in, out, s); } \
+    if (p.na == 2) { XATU_TRY_TC(NVv, NCv, 2) return launch_tile<float, NVv, NCv, 2, true>(p, in, out, s); } \
+    if (p.na == 3) { XATU_TRY_TC(NVv, NCv, 3) return launch_tile<float, NVv, NCv, 3, true>(p, in, out, s); } \
+    if (p.na == 4) { XATU_TRY_TC(NVv, NCv, 4) return launch_tile<float, NVv, NCv, 4, true>(p, in, out, s); } \
   }
   XATU_CASE(1, 1)
   XATU_CASE(1, 2)
@@ -47,6 +88,7 @@ cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, cons
   XATU_CASE(3, 2)
   XATU_CASE(3, 3)
 #undef XATU_CASE
+#undef XATU_TRY_TC
   *launched = false;
   return cudaSuccess;
 }

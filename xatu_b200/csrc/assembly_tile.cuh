@@ -43,12 +43,9 @@ __device__ __forceinline__ void split_store(__nv_bfloat162* hi, __nv_bfloat162* 
 // commutes with negation (hi and lo of -x are -hi and -lo), so the conjugate of a packed value is the same words
 // with the sign bits of the imaginary halves flipped (bit 31 of each word).
 __device__ __forceinline__ uint2 split_pack(float re, float im) {
-  const __nv_bfloat16 hr = __float2bfloat16_rn(re), hi_ = __float2bfloat16_rn(im);
-  __nv_bfloat162 h, l;
-  h.x = hr;
-  h.y = hi_;
-  l.x = __float2bfloat16_rn(re - __bfloat162float(hr));
-  l.y = __float2bfloat16_rn(im - __bfloat162float(hi_));
+  const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);   // one paired conversion, re in the low half
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(re - hf.x, im - hf.y);
   return make_uint2(*reinterpret_cast<const unsigned*>(&h), *reinterpret_cast<const unsigned*>(&l));
 }
 

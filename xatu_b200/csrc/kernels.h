@@ -24,8 +24,9 @@ cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const 
                                  bool force_generic, cudaStream_t s, int* path);
 
 // Single-system tile kernels (assembly_f32.cu / assembly_f64.cu).
+// *tensor_cores: the f32 tile ran its band overlaps on tcgen05 (assembly_tc.cuh).
 cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
-                                   bool* launched);
+                                   bool* launched, bool* tensor_cores);
 cudaError_t xatu_dispatch_tile_f64(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
                                    bool* launched);
 // Batched persistent assembly (assembly_batch.cu), mixed precision, one band-window class per launch.
