@@ -1,7 +1,8 @@
 """Device eigensolver of the Davidson Rayleigh-Ritz step (lowest k eigenpairs of a small Hermitian
 matrix: Householder tridiagonalisation, Sturm multisection, inverse iteration) against numpy's
-eigvalsh on spectra that stress it: random, exactly and nearly degenerate, already diagonal, bordered
-diagonal (the shape of a grown projected matrix), zero, and the largest supported size."""
+eigvalsh on spectra that stress it: random (even and odd sizes), exactly and nearly degenerate, already
+diagonal, bordered diagonal (the shape of a grown projected matrix), zero, and the largest supported
+size."""
 import numpy as np
 import pytest
 
@@ -28,7 +29,7 @@ def _unitary(rng, m):
 def _cases():
     rng = np.random.default_rng(2024)
     out = []
-    for m in (1, 2, 3, 12, 24, 48, 64, 112):
+    for m in (1, 2, 3, 12, 24, 41, 48, 63, 64, 65, 112):
         B = rng.standard_normal((m, m)) + 1j * rng.standard_normal((m, m))
         out.append((f"random{m}", (B + B.conj().T) / 2, min(m, 12)))
     m = 48
