@@ -101,7 +101,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
   DBuf* bufs[] = {&ctx->d_motif, &ctx->d_orboff, &ctx->d_basis, &ctx->d_cellsR, &ctx->d_HR, &ctx->d_SR, &ctx->d_kpoints, &ctx->d_mesh,
                   &ctx->d_cells, &ctx->d_G, &ctx->d_kgrid, &ctx->d_Q, &ctx->d_eigval, &ctx->d_eigvec, &ctx->d_eigvalQ,
                   &ctx->d_eigvecQ, &ctx->d_pairs, &ctx->d_vtab, &ctx->d_vtabX, &ctx->d_table, &ctx->d_VX,
-                  &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status,
+                  &ctx->d_exL, &ctx->d_exR, &ctx->d_H, &ctx->d_Khi, &ctx->d_Klo, &ctx->d_diag, &ctx->d_status, &ctx->d_asmops,
                   &ctx->d_work, &ctx->dv_V, &ctx->dv_W, &ctx->dv_T, &ctx->dv_Y, &ctx->dv_U, &ctx->dv_R,
                   &ctx->dv_X, &ctx->dv_Yf, &ctx->dv_G, &ctx->dv_tmp, &ctx->dv_diagH, &ctx->dv_small,
                   &ctx->dv_norm, &ctx->dv_Bop, &ctx->dv_Blo, &ctx->dv_Uhi, &ctx->dv_Ulo, &ctx->d_adjX, &ctx->d_adjdvtab,
@@ -667,6 +667,8 @@ void xatu_assembly_setup(const xatu_ctx* ctx, const int* basis, AsmParams* pp, A
   in.exR = ctx->d_exR.as<cd>();
   in.status = ctx->d_status.as<int>();
   in.basis = basis;
+  in.tc_ops = nullptr;
+  in.tc_ops_bytes = 0;
   memset(&out, 0, sizeof(out));
   out.H = ctx->d_H.as<cd>();
   out.Khi = ctx->d_Khi.as<__nv_bfloat162>();
@@ -699,6 +701,15 @@ static xatu_status build_impl(xatu_ctx* ctx, int precision, const int* basis) {
   AsmInputs in;
   AsmOutputs out;
   xatu_assembly_setup(ctx, basis, &p, &in, &out);
+  if (mixed && basis == nullptr) {
+    // scratch for the operand images of the tensor-core tile (none when the band window does not take it)
+    const size_t ops = xatu_assembly_tc_scratch_bytes(p);
+    if (ops) {
+      XATU_CK(ctx->d_asmops.ensure(ops));
+      in.tc_ops = ctx->d_asmops.as<unsigned char>();
+      in.tc_ops_bytes = ops;
+    }
+  }
   XATU_CK(cudaEventRecord(ctx->ev[4], ctx->stream));
   if (ctx->exchange) {
     const int blocks = (int)((N + 127) / 128);

@@ -30,12 +30,52 @@ static cudaError_t launch_tile_tc(const AsmParams& p, const AsmInputs& in, const
   const int ntiles = nblk * (nblk + 1) / 2;
   const AsmTcGeom g = asm_tc_geom<NV, NC, NA, TK>(p.norb);
   if (g.KP > XATU_ASM_TC_KPMAX || g.bytes > 200 * 1024) return cudaErrorNotSupported;
+  const AsmTcImage im = asm_tc_image<NV, NC, NA, TK>(g);
+  if (!in.tc_ops || in.tc_ops_bytes < (size_t)nblk * im.block) return cudaErrorNotSupported;
+  // operand images of every k block, then the tiles
+  const long long items = (long long)nblk * TK * (NV + NC) * (g.KP / 8);
+  asm_tc_format_kernel<NV, NC, NA, TK><<<(unsigned)((items + 255) / 256), 256, 0, s>>>(p, in, nblk);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   auto kern = bse_assemble_tile_tc_kernel<NV, NC, NA, TK>;
-  cudaError_t e = xatu_raise_smem_limit((const void*)kern, g.bytes);
+  e = xatu_raise_smem_limit((const void*)kern, g.bytes);
   if (e != cudaSuccess) return e;
   kern<<<ntiles, asm_tc_threads(TK), g.bytes, s>>>(p, in, out, nblk);
   return cudaGetLastError();
   }
+}
+
+template <int NV, int NC, int NA>
+static size_t tc_scratch(const AsmParams& p) {
+  constexpr int TK = (NV * NC <= 4) ? 16 : 8;
+  if constexpr (NA * TK * NC > 128 || NA * TK * NV > 128 || 2 * TK * (NV + NC) > 256) {
+    return 0;
+  } else {
+    const AsmTcGeom g = asm_tc_geom<NV, NC, NA, TK>(p.norb);
+    if (g.KP > XATU_ASM_TC_KPMAX) return 0;
+    return (size_t)((p.nk + TK - 1) / TK) * asm_tc_image<NV, NC, NA, TK>(g).block;
+  }
+}
+
+size_t xatu_assembly_tc_scratch_bytes(const AsmParams& p) {
+#define XATU_CASE(NVv, NCv)                                 \
+  if (p.nv == NVv && p.nc == NCv) {                         \
+    if (p.na == 1) return tc_scratch<NVv, NCv, 1>(p);       \
+    if (p.na == 2) return tc_scratch<NVv, NCv, 2>(p);       \
+    if (p.na == 3) return tc_scratch<NVv, NCv, 3>(p);       \
+    if (p.na == 4) return tc_scratch<NVv, NCv, 4>(p);       \
+  }
+  XATU_CASE(1, 1)
+  XATU_CASE(1, 2)
+  XATU_CASE(1, 3)
+  XATU_CASE(2, 1)
+  XATU_CASE(2, 2)
+  XATU_CASE(2, 3)
+  XATU_CASE(3, 1)
+  XATU_CASE(3, 2)
+  XATU_CASE(3, 3)
+#undef XATU_CASE
+  return 0;
 }
 
 template <typename T, int NV, int NC, int NA, bool MIXED>

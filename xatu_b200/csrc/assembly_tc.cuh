@@ -16,7 +16,10 @@
 //   D[(a, k', band')][(k, band)] = Re, D[...][TK nband + (k, band)] = Im.
 // KP = 2 norb rounded up to 16.  Operands are split FP16 (x = hi + lo, 22 significant bits: |C| <= 1 keeps
 // them in range) and each overlap is hi*hi + hi*lo + lo*hi, so rho carries FP32-level accuracy.
-// Shared-memory operands use the no-swizzle K-major layout of 8-row x 16-byte core matrices.
+// Shared-memory operands use the no-swizzle K-major layout of 8-row x 16-byte core matrices.  Both operand
+// kinds of every k block are formatted once per build (asm_tc_format_kernel) into images in global memory
+// laid out exactly as the tile needs them in shared memory, so a tile stages its operands with four bulk
+// copies (cp.async.bulk, completion on an mbarrier) and no conversion work.
 //
 // The accumulators are moved to shared memory (k side first, so that the per-pair reads below are contiguous
 // across the threads of a warp; the block has at least 128 threads, one warp per tensor-memory sub-partition),
@@ -83,6 +86,25 @@ __host__ __device__ inline AsmTcGeom asm_tc_geom(int norb) {
   g.off_ex = end;
   g.bytes = g.off_ex + (size_t)2 * TR * NA * 8;
   return g;
+}
+
+// Operand images of one k block in global memory: A1 (hi, lo planes), A2, B1, B2, the same bytes as the
+// tile's shared-memory planes (the A images built from the block's k points as the k' side, the B images as
+// the k side).
+struct AsmTcImage {
+  size_t A1, A2, B1, B2;   // byte offsets inside a block's image
+  size_t block;            // bytes per k block
+};
+
+template <int NV, int NC, int NA, int TK>
+__host__ __device__ inline AsmTcImage asm_tc_image(const AsmTcGeom& g) {
+  AsmTcImage im;
+  im.A1 = 0;
+  im.A2 = im.A1 + 2 * g.opA1_plane;
+  im.B1 = im.A2 + 2 * g.opA2_plane;
+  im.B2 = im.B1 + 2 * g.opB1_plane;
+  im.block = (im.B2 + 2 * g.opB2_plane + 127) & ~(size_t)127;
+  return im;
 }
 
 __device__ __forceinline__ uint32_t asm_smem_u32(const void* p) {
@@ -155,6 +177,87 @@ __device__ __forceinline__ uint32_t asm_op_off(int r, int k, int sbo) {
   return (uint32_t)((r >> 3) * sbo + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// Operand images of every k block (one thread per group of 4 orbitals of one band at one k): the A form
+// (atom-masked rows (atom, k, band), [Re, Im]) and the two B forms (rows (k, band): [Re, Im] and the
+// imaginary-part form, [-Im, Re] for conduction bands (rho1), [Im, -Re] for valence bands (rho2)).
+template <int NV, int NC, int NA, int TK>
+__global__ void asm_tc_format_kernel(AsmParams p, AsmInputs in, int nblk) {
+  constexpr int NB = NV + NC;
+  constexpr int TKC = TK * NC, TKV = TK * NV;
+  const AsmTcGeom G = asm_tc_geom<NV, NC, NA, TK>(p.norb);
+  const AsmTcImage IM = asm_tc_image<NV, NC, NA, TK>(G);
+  const int norb = p.norb, NQ = G.KP / 8;
+  const long long total = (long long)nblk * TK * NB * NQ;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t % NQ);
+    const long long r = t / NQ;
+    const int band = (int)(r % NB);
+    const int kq = (int)((r / NB) % TK);
+    const int blk = (int)(r / (NB * TK));
+    const int kg = blk * TK + kq;
+    float re[4], im[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      re[j] = 0.f;
+      im[j] = 0.f;
+      const int o = 4 * q + j;
+      if (kg < p.nk && o < norb) {
+        const cd c = (band < NV ? in.eigvec : in.eigvecQ)[((int64_t)kg * p.nb + band) * norb + o];
+        re[j] = (float)c.x;
+        im[j] = (float)c.y;
+      }
+    }
+    const bool cond = band >= NV;
+    const int bb = cond ? band - NV : band;
+    unsigned char* img = in.tc_ops + (size_t)blk * IM.block;
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) asm_split_f16x2(re[j], im[j], h[j], l[j]);
+    {
+      // A form, one row per atom
+      unsigned char* base = img + (cond ? IM.A1 : IM.A2);
+      const size_t plane = cond ? G.opA1_plane : G.opA2_plane;
+      const int nbw = cond ? NC : NV;
+#pragma unroll
+      for (int a = 0; a < NA; a++) {
+        uint32_t hm[4], lm[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int o = 4 * q + j;
+          const bool own = o >= p.orb_off[a] && o < p.orb_off[a + 1];
+          hm[j] = own ? h[j] : 0u;
+          lm[j] = own ? l[j] : 0u;
+        }
+        const uint32_t off = asm_op_off((a * TK + kq) * nbw + bb, 8 * q, G.sbo);
+        *reinterpret_cast<uint4*>(base + off) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
+        *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
+      }
+    }
+    {
+      // B forms
+      unsigned char* base = img + (cond ? IM.B1 : IM.B2);
+      const size_t plane = cond ? G.opB1_plane : G.opB2_plane;
+      const int row = kq * (cond ? NC : NV) + bb;
+      uint32_t off = asm_op_off(row, 8 * q, G.sbo);
+      *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(l[0], l[1], l[2], l[3]);
+#pragma unroll
+      for (int j = 0; j < 4; j++) asm_split_f16x2(cond ? -im[j] : im[j], cond ? re[j] : -re[j], h[j], l[j]);
+      off = asm_op_off(row + (cond ? TKC : TKV), 8 * q, G.sbo);
+      *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+  }
+}
+
+__device__ __forceinline__ void asm_bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   asm_smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(asm_smem_u32(bar))
+               : "memory");
+}
+
 template <int NV, int NC, int NA, int TK>
 __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out,
                                                  int nblk, int tile) {
@@ -171,7 +274,7 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
 #define TIDX(r, c) ((r) * LDT + (SWZ ? ((c) ^ (((r) >> 2) & 15)) : (c)))
   using E = cplx<float>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ uint64_t s_mma_done;
+  __shared__ uint64_t s_mma_done, s_ops_done;
   __shared__ uint32_t s_tmem;
   const AsmTcGeom G = asm_tc_geom<NV, NC, NA, TK>(p.norb);
   int kb, kb2;
@@ -204,74 +307,25 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_mma_done)), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_ops_done)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
 
-  // ---- operands: two threads per (side, k, band), each filling every other group of 4 orbitals (8 K values
-  //      = one 16-byte core-matrix row)
-  {
-    const int NQ = G.KP / 8;
-    for (int w = tid; w < 4 * TK * NB; w += blockDim.x) {
-      const int combo = w >> 1;
-      const int band = combo % NB;
-      const int kq = (combo / NB) % TK;
-      const int side = combo / (NB * TK);   // 0: k side (B operands), 1: k' side (A operands)
-      const int kg = (side ? kb2 : kb) * TK + kq;
-      const bool cond = band >= NV;
-      const int bb = cond ? band - NV : band;
-      const cd* src = (band < NV ? in.eigvec : in.eigvecQ) + ((int64_t)kg * p.nb + band) * norb;
-      for (int q = w & 1; q < NQ; q += 2) {
-        float re[4], im[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          re[j] = 0.f;
-          im[j] = 0.f;
-          const int o = 4 * q + j;
-          if (kg < p.nk && o < norb) {
-            const cd c = src[o];
-            re[j] = (float)c.x;
-            im[j] = (float)c.y;
-          }
-        }
-        uint32_t h[4], l[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) asm_split_f16x2(re[j], im[j], h[j], l[j]);
-        if (side == 1) {
-          // A rows (atom, k', band'): the atom's own orbitals only
-          unsigned char* base = smem_raw + (cond ? G.off_A1 : G.off_A2);
-          const size_t plane = cond ? G.opA1_plane : G.opA2_plane;
-          const int nbw = cond ? NC : NV;
-#pragma unroll
-          for (int a = 0; a < NA; a++) {
-            uint32_t hm[4], lm[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const int o = 4 * q + j;
-              const bool own = o >= p.orb_off[a] && o < p.orb_off[a + 1];
-              hm[j] = own ? h[j] : 0u;
-              lm[j] = own ? l[j] : 0u;
-            }
-            const uint32_t off = asm_op_off((a * TK + kq) * nbw + bb, 8 * q, G.sbo);
-            *reinterpret_cast<uint4*>(base + off) = make_uint4(hm[0], hm[1], hm[2], hm[3]);
-            *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(lm[0], lm[1], lm[2], lm[3]);
-          }
-        } else {
-          // B rows (k, band) in the real-part form [Re, Im] and the imaginary-part form
-          // ([-Im, Re] for rho1, [Im, -Re] for rho2)
-          unsigned char* base = smem_raw + (cond ? G.off_B1 : G.off_B2);
-          const size_t plane = cond ? G.opB1_plane : G.opB2_plane;
-          const int row = kq * (cond ? NC : NV) + bb;
-          uint32_t off = asm_op_off(row, 8 * q, G.sbo);
-          *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(l[0], l[1], l[2], l[3]);
-#pragma unroll
-          for (int j = 0; j < 4; j++) asm_split_f16x2(cond ? -im[j] : im[j], cond ? re[j] : -re[j], h[j], l[j]);
-          off = asm_op_off(row + (cond ? TKC : TKV), 8 * q, G.sbo);
-          *reinterpret_cast<uint4*>(base + off) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4*>(base + plane + off) = make_uint4(l[0], l[1], l[2], l[3]);
-        }
-      }
-    }
+  // ---- operands: the A images of block kb2 (the k' side) and the B images of block kb (the k side), four bulk
+  //      copies into the planes of the shared-memory layout; only the thread that issues the products waits
+  if (tid == 0) {
+    const AsmTcImage IM = asm_tc_image<NV, NC, NA, TK>(G);
+    const unsigned char* ia = in.tc_ops + (size_t)kb2 * IM.block;
+    const unsigned char* ib = in.tc_ops + (size_t)kb * IM.block;
+    const uint32_t bA1 = (uint32_t)(2 * G.opA1_plane), bA2 = (uint32_t)(2 * G.opA2_plane);
+    const uint32_t bB1 = (uint32_t)(2 * G.opB1_plane), bB2 = (uint32_t)(2 * G.opB2_plane);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(asm_smem_u32(&s_ops_done)),
+                 "r"(bA1 + bA2 + bB1 + bB2)
+                 : "memory");
+    asm_bulk_load(smem_raw + G.off_A1, ia + IM.A1, bA1, &s_ops_done);
+    asm_bulk_load(smem_raw + G.off_A2, ia + IM.A2, bA2, &s_ops_done);
+    asm_bulk_load(smem_raw + G.off_B1, ib + IM.B1, bB1, &s_ops_done);
+    asm_bulk_load(smem_raw + G.off_B2, ib + IM.B2, bB2, &s_ops_done);
   }
   // exchange factors of the tile's rows and columns
   const int64_t row0 = (int64_t)kb * TR, col0 = (int64_t)kb2 * TR;
@@ -293,15 +347,19 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
       sR[t] = rr;
     }
   }
-  // generic-proxy stores must be visible to the tensor core (async proxy)
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
 
-  // ---- the two overlap products, issued by one thread
+  // ---- the two overlap products, issued by one thread once the operand copies have landed
+  bool ops_ok = true;
   if (tid == 0) {
+    ops_ok = asm_mbar_wait(&s_ops_done, 0);
+    // copies still in flight must land before this block's shared memory is released
+    if (!ops_ok) asm_mbar_wait(&s_ops_done, 0);
+  }
+  if (tid == 0 && ops_ok) {
     constexpr uint32_t id1 = asm_idesc_f16(N1), id2 = asm_idesc_f16(N2);
     const uint32_t d1 = tmem, d2 = tmem + N1;
     const unsigned char* A1 = smem_raw + G.off_A1;
@@ -325,7 +383,8 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
                      asm_smem_u32(&s_mma_done))
                  : "memory");
   }
-  const bool mma_ok = __syncthreads_and(asm_mbar_wait(&s_mma_done, 0) ? 1 : 0);
+  // (on a failed operand wait no product was issued and nothing will arrive: skip the wait)
+  const bool mma_ok = __syncthreads_and(ops_ok ? 1 : 0) && __syncthreads_and(asm_mbar_wait(&s_mma_done, 0) ? 1 : 0);
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (!mma_ok) {
     if (tid == 0) atomicOr(in.status, XATU_DEVERR_NOCONV);

@@ -79,6 +79,7 @@ struct xatu_ctx {
   DBuf d_eigval, d_eigvec, d_eigvalQ, d_eigvecQ;
   DBuf d_pairs, d_vtab, d_vtabX, d_table, d_VX, d_exL, d_exR;
   DBuf d_H, d_Khi, d_Klo, d_diag, d_status;
+  DBuf d_asmops;   // operand images of the tensor-core assembly tile
   DBuf d_work;       // solver scratch
   int last_assembly_path = -1;
 

@@ -59,6 +59,8 @@ struct AsmInputs {
   const cd* exR;           // N x na
   int* status;             // device error word
   const int* basis;        // NULL, or N x 3 (k, valence column, conduction index) of a caller-given basis
+  unsigned char* tc_ops;   // NULL, or scratch for the tensor-core tile's operand images (assembly_tc.cuh)
+  size_t tc_ops_bytes;
 };
 
 struct AsmOutputs {
