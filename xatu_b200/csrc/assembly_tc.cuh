@@ -467,13 +467,29 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
 #pragma unroll
           for (int v = 0; v < NV; v++) cfma(Tm[a][v2][v], Vr[a][b], rho2[v2][v]);
     }
+    // rho1_a(c, c') of this pair (for two conduction bands the pair's two c' values are one 16-byte word)
+    E rho1c[NA][NC][NC];
+#pragma unroll
+    for (int a = 0; a < NA; a++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const E* src = r1 + ((size_t)a * TKC + kk * NC + c) * TKC + kk2 * NC;
+        if constexpr (NC == 2) {
+          const float4 w = *reinterpret_cast<const float4*>(src);
+          rho1c[a][c][0] = {w.x, w.y};
+          rho1c[a][c][1] = {w.z, w.w};
+        } else {
+#pragma unroll
+          for (int c2 = 0; c2 < NC; c2++) rho1c[a][c][c2] = src[c2];
+        }
+      }
 #pragma unroll
     for (int c = 0; c < NC; c++) {
 #pragma unroll
       for (int c2 = 0; c2 < NC; c2++) {
         E rho1[NA];
 #pragma unroll
-        for (int a = 0; a < NA; a++) rho1[a] = r1[((size_t)a * TKC + kk * NC + c) * TKC + kk2 * NC + c2];
+        for (int a = 0; a < NA; a++) rho1[a] = rho1c[a][c][c2];
 #pragma unroll
         for (int v = 0; v < NV; v++) {
 #pragma unroll
@@ -517,10 +533,28 @@ __device__ __forceinline__ void assemble_tile_tc(const AsmParams& p, const AsmIn
     __syncthreads();   // every thread has read its overlaps: the staging tile may overwrite them
     if (active) {
 #pragma unroll
-      for (int pi = 0; pi < NCV; pi++)
+      for (int pi = 0; pi < NCV; pi++) {
+        if constexpr (NCV % 2 != 0) {
 #pragma unroll
-        for (int pj = 0; pj < NCV; pj++)
-          if (!(k == k2 && pj < pi)) sT2[TIDX(kk * NCV + pi, kk2 * NCV + pj)] = held[APART ? 0 : pi * NCV + pj];
+          for (int pj = 0; pj < NCV; pj++)
+            if (!(k == k2 && pj < pi)) sT2[TIDX(kk * NCV + pi, kk2 * NCV + pj)] = held[APART ? 0 : pi * NCV + pj];
+        } else {
+          // two neighbouring columns per 16-byte store where the swizzle keeps them adjacent (XOR of a
+          // multiple of 4 with an even column moves both together)
+#pragma unroll
+          for (int pj = 0; pj < NCV; pj += 2) {
+            const int r = kk * NCV + pi, c0 = kk2 * NCV + pj;
+            const uint2 u0 = held[APART ? 0 : pi * NCV + pj], u1 = held[APART ? 0 : pi * NCV + pj + 1];
+            const bool w0 = !(k == k2 && pj < pi), w1 = !(k == k2 && pj + 1 < pi);
+            if (w0 && w1 && ((TIDX(r, c0) & 1) == 0) && TIDX(r, c0 + 1) == TIDX(r, c0) + 1) {
+              *reinterpret_cast<uint4*>(&sT2[TIDX(r, c0)]) = make_uint4(u0.x, u0.y, u1.x, u1.y);
+            } else {
+              if (w0) sT2[TIDX(r, c0)] = u0;
+              if (w1) sT2[TIDX(r, c0 + 1)] = u1;
+            }
+          }
+        }
+      }
     }
   }
   __syncthreads();
