@@ -110,9 +110,10 @@ def hx_operand_rows(nstates: int) -> int:
     return 2 * ((min(b, 24) + 7) // 8 * 8)
 
 
-# DRAM traffic of the Hermitian K.X product per stored element, from one ncu capture of the kernel at
-# N = 5184 (k mesh 36 x 36, stored planes 108 MB, operands and Y in L2); None until captured
-HX_TRAFFIC_PER_STORED_ELEMENT = None
+# DRAM traffic of the Hermitian K.X product per stored element (read + write), from a one-pass ncu capture
+# of three launches at N = 9216 (k mesh 48 x 48, 43.06 M stored elements, 350.6 MB read, 0.3 - 0.7 MB
+# written): 8.149 - 8.160 B.  The product streams K once, so the traffic grows with the stored elements.
+HX_TRAFFIC_PER_STORED_ELEMENT = 8.153
 
 
 class ClockSampler:
