@@ -305,8 +305,8 @@ xatu_status xatu_stage_times(const xatu_ctx *ctx, float *ms4);
 /* Device time of one kernel family measured with CUDA events on the context's stream: which = 0 the BSE
    assembly (last build), 1 the K.X products of the last Davidson solve, 2 the last xatu_adjoint call (first
    to last launch), 3 its pair kernel.  *path: for the K.X products 1 CUDA cores, 2 tcgen05; for the assembly
-   0 tile kernel on CUDA cores, 1 element-wise kernel, 2 tile kernel with the band overlaps on tcgen05; 0 where
-   it does not apply. */
+   0 tile kernel on CUDA cores, 1 element-wise kernel, 2 tile kernel with the band overlaps on tcgen05, 3 row-panel
+   kernel with the band overlaps on tcgen05; 0 where it does not apply. */
 xatu_status xatu_kernel_stats(const xatu_ctx *ctx, int which, int64_t *launches, double *total_ms, int *path);
 /* Number of engine kernels launched on this context since creation. */
 xatu_status xatu_kernel_launches(const xatu_ctx *ctx, int64_t *count);

@@ -323,24 +323,34 @@ def test_reciprocal_exchange_16_states_vs_oracle():
     assert np.abs(res.eigval - w).max() < ENERGY_TOL
 
 
-@pytest.mark.parametrize("model,ncell,nbands,kw", [
-    ("MoS2.model", 10, 2, dict(Q=(0, 0.1, 0), exchange=True)),                 # 2v + 2c, tiles of 16 k points
-    ("MoS2.model", 5, 3, dict(exchange=True)),                                  # 3v + 3c, tiles of 8 k points
-    ("hBN.model", 14, 1, dict(mode="reciprocalspace", nG=3, exchange=True)),    # 1v + 1c, reciprocal space
+@pytest.mark.parametrize("model,ncell,nbands,kw,panel", [
+    # 2v + 2c: row panels of 64 k points (the second one partial) and column tiles of 8 (the last one partial)
+    ("MoS2.model", 10, 2, dict(Q=(0, 0.1, 0), exchange=True), True),
+    ("MoS2.model", 5, 3, dict(exchange=True), False),                                # 3v + 3c: tensor-core tile
+    ("hBN.model", 14, 1, dict(mode="reciprocalspace", nG=3, exchange=True), True),   # 1v + 1c, reciprocal space
+    ("MoS2.model", 9, 1, dict(bands=[0, 1, 2]), True),                               # 1v + 2c
+    ("MoS2.model", 9, 1, dict(bands=[-1, 0, 1], exchange=True), True),               # 2v + 1c
 ])
-def test_tensor_core_assembly(model, ncell, nbands, kw, monkeypatch):
-    """The mixed build with the band overlaps on tcgen05 (assembly path 2) against the oracle's FP64 matrix and
-    against the CUDA-core tile (path 0) on the same band stacks."""
+def test_tensor_core_assembly(model, ncell, nbands, kw, panel, monkeypatch):
+    """The mixed build with the band overlaps on tcgen05 (assembly path 3: row panels, path 2: tiles) against the
+    oracle's FP64 matrix, and the three mixed kernels (row panels, tensor-core tile, CUDA-core tile, path 0)
+    against each other on the same band stacks."""
     cfg = model_config(model)
     params = [1., 4., 13.55] if model == "MoS2.model" else [1, 1, 10]
     ex, orc = _pair(cfg, ncell, nbands, params, **kw)
     ex.upload_bands(orc.eigval, orc.eigvec, orc.eigvalQ, orc.eigvecQ)
     ex.BShamiltonian("mixed")
-    assert ex.kernelStats("assembly")[2] == 2
+    assert ex.kernelStats("assembly")[2] == (3 if panel else 2)
     H_tc = ex.HBS
     Ho = orc.bs_hamiltonian()
     assert rel_err(H_tc, Ho) < MIXED_TOL
     assert np.array_equal(H_tc, H_tc.conj().T)
+    if panel:
+        monkeypatch.setenv("XATU_ASSEMBLY_TILE_TC", "1")
+        ex.BShamiltonian("mixed")
+        assert ex.kernelStats("assembly")[2] == 2
+        assert rel_err(ex.HBS, H_tc) < MIXED_TOL
+        monkeypatch.delenv("XATU_ASSEMBLY_TILE_TC")
     monkeypatch.setenv("XATU_ASSEMBLY_CUDA_CORE", "1")
     ex.BShamiltonian("mixed")
     assert ex.kernelStats("assembly")[2] == 0

@@ -84,12 +84,13 @@ static cudaError_t launch_generic(const AsmParams& p, const AsmInputs& in, const
   return cudaGetLastError();
 }
 
-// *path: 0 tile kernel (CUDA cores), 1 generic kernel, 2 tile kernel with the band overlaps on tcgen05.
+// *path: 0 tile kernel (CUDA cores), 1 generic kernel, 2 tile kernel with the band overlaps on tcgen05, 3 row-panel
+// kernel with the band overlaps on tcgen05.
 cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, bool mixed,
                                  bool force_generic, cudaStream_t s, int* path) {
   if (!force_generic && in.basis == nullptr) {
-    bool launched = false, tc = false;
-    cudaError_t e = mixed ? xatu_dispatch_tile_f32(p, in, out, s, &launched, &tc)
+    bool launched = false, tc = false, panel = false;
+    cudaError_t e = mixed ? xatu_dispatch_tile_f32(p, in, out, s, &launched, &tc, &panel)
                           : xatu_dispatch_tile_f64(p, in, out, s, &launched);
     if (e == cudaErrorNotSupported) {
       cudaGetLastError();
@@ -98,7 +99,7 @@ cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const 
       return e;
     }
     if (launched) {
-      *path = tc ? 2 : 0;
+      *path = panel ? 3 : tc ? 2 : 0;
       return cudaSuccess;
     }
   }

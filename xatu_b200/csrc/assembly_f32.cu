@@ -1,11 +1,14 @@
-// Single-system tile assembly, float: one CTA per upper-triangular (k-block, k'-block) tile.  Tile side 16 k
-// points for windows of up to 4 e-h pairs per k, 8 for larger windows (the staging tile grows with (nv nc)^2).
-// The band overlaps run on the tensor cores (assemble_tile_tc, assembly_tc.cuh) when the orbital basis and
-// the window fit its products; otherwise, or with XATU_ASSEMBLY_CUDA_CORE=1 in the environment, on the CUDA
-// cores (assemble_tile, assembly_tile.cuh).
+// Single-system assembly, float (mixed precision).  Three kernels, tried in this order:
+//  * the persistent row-panel kernel (assembly_panel.cuh): band windows of up to 2 valence and 2 conduction
+//    bands, the band overlaps on the tensor cores read straight from tensor memory;
+//  * the tile kernel with the overlaps on the tensor cores (assemble_tile_tc, assembly_tc.cuh): one CTA per
+//    upper-triangular (k-block, k'-block) tile, tile side 16 k points for windows of up to 4 e-h pairs per k,
+//    8 for larger windows;
+//  * the same tile on the CUDA cores (assemble_tile, assembly_tile.cuh).
+// XATU_ASSEMBLY_CUDA_CORE=1 in the environment selects the last, XATU_ASSEMBLY_TILE_TC=1 the second.
 #include <cstdlib>
 
-#include "assembly_tc.cuh"
+#include "assembly_panel.cuh"
 
 template <typename T, int NV, int NC, int NA, bool MIXED, int TK>
 __global__ void __launch_bounds__(TK * TK)
@@ -45,16 +48,64 @@ static cudaError_t launch_tile_tc(const AsmParams& p, const AsmInputs& in, const
   }
 }
 
+static int panel_num_sms() {
+  static int cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cached[dev] = n > 0 ? n : 148;
+  }
+  return cached[dev];
+}
+
+// Row-panel kernel: operand images, FP32 table and k coordinates, the persistent assembly, the diagonal blocks'
+// lower triangles.
+template <int NV, int NC, int NA>
+static cudaError_t launch_panel(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s) {
+  if constexpr (!PanelShape<NV, NC, NA>::SUPPORTED) {
+    return cudaErrorNotSupported;
+  } else {
+    AsmPanelGeom g;
+    if (!asm_panel_geom<NV, NC, NA>(p, g)) return cudaErrorNotSupported;
+    if (!in.tc_ops || in.tc_ops_bytes < g.bytes) return cudaErrorNotSupported;
+    auto kern = bse_assemble_panel_kernel<NV, NC, NA>;
+    // the register split of the warpgroups needs the full launch allotment (setmaxnreg.inc would wait forever
+    // on a smaller pool)
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void*)kern);
+    if (e != cudaSuccess) return e;
+    if (fa.numRegs != XATU_PANEL_REGS_LAUNCH) return cudaErrorNotSupported;
+    e = xatu_raise_smem_limit((const void*)kern, g.smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(in.tc_ops + g.img_F, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    asm_panel_format_kernel<NV, NC, NA><<<4 * panel_num_sms(), 256, 0, s>>>(p, in, g);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int grid = g.total < panel_num_sms() ? g.total : panel_num_sms();
+    kern<<<grid, XATU_PANEL_THREADS, g.smem, s>>>(p, in, out, g);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const unsigned nd = (unsigned)((p.N + XATU_KBLOCK - 1) / XATU_KBLOCK);
+    asm_diag_mirror_kernel<<<dim3(nd, 10), dim3(32, 8), 0, s>>>(reinterpret_cast<unsigned*>(out.Khi),
+                                                               reinterpret_cast<unsigned*>(out.Klo), p.N, p.ldk);
+    return cudaGetLastError();
+  }
+}
+
 template <int NV, int NC, int NA>
 static size_t tc_scratch(const AsmParams& p) {
   constexpr int TK = (NV * NC <= 4) ? 16 : 8;
-  if constexpr (NA * TK * NC > 128 || NA * TK * NV > 128 || 2 * TK * (NV + NC) > 256) {
-    return 0;
-  } else {
+  size_t bytes = 0;
+  if constexpr (!(NA * TK * NC > 128 || NA * TK * NV > 128 || 2 * TK * (NV + NC) > 256)) {
     const AsmTcGeom g = asm_tc_geom<NV, NC, NA, TK>(p.norb);
-    if (g.KP > XATU_ASM_TC_KPMAX) return 0;
-    return (size_t)((p.nk + TK - 1) / TK) * asm_tc_image<NV, NC, NA, TK>(g).block;
+    if (g.KP <= XATU_ASM_TC_KPMAX) bytes = (size_t)((p.nk + TK - 1) / TK) * asm_tc_image<NV, NC, NA, TK>(g).block;
   }
+  AsmPanelGeom pg;
+  if (asm_panel_geom<NV, NC, NA>(p, pg) && pg.bytes > bytes) bytes = pg.bytes;
+  return bytes;
 }
 
 size_t xatu_assembly_tc_scratch_bytes(const AsmParams& p) {
@@ -97,13 +148,25 @@ static cudaError_t launch_tile(const AsmParams& p, const AsmInputs& in, const As
 
 // Launches the tile kernel of the band-window class of p; *launched = false when the class has none.
 cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
-                          bool* launched, bool* tensor_cores) {
+                          bool* launched, bool* tensor_cores, bool* panel) {
   *launched = true;
   *tensor_cores = false;
+  *panel = false;
   const char* cc = std::getenv("XATU_ASSEMBLY_CUDA_CORE");
   const bool allow_tc = !(cc && cc[0] == '1');
-  // the tensor-core tile first; cudaErrorNotSupported (orbital basis or staging too large) falls back
+  const char* tt = std::getenv("XATU_ASSEMBLY_TILE_TC");
+  const bool allow_panel = allow_tc && !(tt && tt[0] == '1');
+  // the row-panel kernel, then the tensor-core tile; cudaErrorNotSupported (band window, orbital basis or
+  // staging too large) falls back
 #define XATU_TRY_TC(NVt, NCt, NAt)                                                           \
+  if (allow_panel) {                                                                         \
+    cudaError_t e = launch_panel<NVt, NCt, NAt>(p, in, out, s);                               \
+    if (e != cudaErrorNotSupported) {                                                        \
+      *tensor_cores = e == cudaSuccess;                                                      \
+      *panel = e == cudaSuccess;                                                             \
+      return e;                                                                              \
+    }                                                                                        \
+  }                                                                                          \
   if (allow_tc) {                                                                            \
     cudaError_t e = launch_tile_tc<NVt, NCt, NAt>(p, in, out, s);                             \
     if (e != cudaErrorNotSupported) {                                                        \

@@ -24,12 +24,12 @@ cudaError_t xatu_launch_assembly(const AsmParams& p, const AsmInputs& in, const 
                                  bool force_generic, cudaStream_t s, int* path);
 
 // Single-system tile kernels (assembly_f32.cu / assembly_f64.cu).
-// Bytes of operand-image scratch (AsmInputs::tc_ops) the tensor-core tile of p's class needs; 0 when the class
-// does not take that tile.
+// Bytes of operand-image scratch (AsmInputs::tc_ops) the tensor-core kernels of p's class need (row panels or
+// tiles, whichever needs more); 0 when the class takes neither.
 size_t xatu_assembly_tc_scratch_bytes(const AsmParams& p);
-// *tensor_cores: the f32 tile ran its band overlaps on tcgen05 (assembly_tc.cuh).
+// *tensor_cores: the band overlaps ran on tcgen05; *panel: in the row-panel kernel (assembly_panel.cuh).
 cudaError_t xatu_dispatch_tile_f32(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
-                                   bool* launched, bool* tensor_cores);
+                                   bool* launched, bool* tensor_cores, bool* panel);
 cudaError_t xatu_dispatch_tile_f64(const AsmParams& p, const AsmInputs& in, const AsmOutputs& out, cudaStream_t s,
                                    bool* launched);
 // Batched persistent assembly (assembly_batch.cu), mixed precision, one band-window class per launch.
