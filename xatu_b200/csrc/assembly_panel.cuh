@@ -24,7 +24,7 @@
 //
 // Pipeline, one CTA per SM: each CTA takes an equal contiguous range of the (panel, tile) pairs that reach the
 // stored upper block triangle (xatu_kstored).  One thread stages the operand images with bulk copies (the
-// panel's A once per panel, each tile's B into a ring of three stages), two more issue the two products into one
+// panel's A once per panel, each tile's B into a ring of three stages), three more issue the products into one
 // of two tensor-memory slots; sixteen consumer warps (four per sub-partition, two k' each) read a slot, release it
 // and combine while the next tile's products run.  The warpgroup of the copy and product threads hands
 // registers to the consumers (setmaxnreg).  Every wait is bounded; on a timeout the CTA records
@@ -37,7 +37,7 @@
 
 #define XATU_PANEL_TKC 8                                  // k' points per column tile
 #define XATU_PANEL_NCW 16                                 // consumer warps (four warpgroups)
-#define XATU_PANEL_THREADS (XATU_PANEL_NCW * 32 + 128)   // + one warpgroup: the copy warp, two product warps, one idle
+#define XATU_PANEL_THREADS (XATU_PANEL_NCW * 32 + 128)   // + one warpgroup: the copy warp and three product warps
 // Registers per thread after the split: the block is launched with 96 per thread (640 threads, one block per SM);
 // the copy/product warpgroup gives back down to 32, the consumer warpgroups take 112: 128 x 32 + 512 x 112 = 640 x 96.
 #define XATU_PANEL_REGS_LAUNCH 96
@@ -367,8 +367,10 @@ __device__ __forceinline__ void panel_next(PanelIter& it, int ntile) {
 }
 
 // Completion barriers of the tiles' products: a ring of XATU_PANEL_NDONE (a multiple of both the operand stages
-// and the tensor-memory slots), tile t -> done[t mod NDONE], phase t / NDONE; both product threads commit to it.
+// and the tensor-memory slots), tile t -> done[t mod NDONE], phase t / NDONE; every product thread commits to it.
 #define XATU_PANEL_NDONE 6
+#define XATU_PANEL_NISSUE 3   // product-issuing threads (warps NCW + 1 ...)
+static_assert(XATU_PANEL_NISSUE >= 1 && XATU_PANEL_NISSUE <= 3, "the issuers share the fifth warpgroup with the copier");
 
 // The thread that stages the operands: the panel's A image once per panel (after every product of the previous
 // panel has completed), each tile's B image into the ring of NBS stages (after the products of the tile that
@@ -412,31 +414,34 @@ __device__ __forceinline__ void panel_copier(const AsmPanelGeom& g, const unsign
   if (nA > 0) asm_mbar_wait(afull, (nA - 1) & 1);
 }
 
-// A thread that issues one of the two overlap products (PR = 0: rho1, 1: rho2) of each tile into its tensor-memory
-// slot; two such threads, on different SM sub-partitions, issue the two products side by side.  The shared-memory
-// descriptors of the product's atoms are formed once, for stage 0, in a small table: a tile adds its stage offset
-// to the B descriptors, each further K step of an atom 256 bytes to both.  One commit per tile to its done
-// barrier.
-template <int NV, int NC, int NA, int PR>
+// Threads that issue the products of each tile into its tensor-memory slot: the (product, atom) chains c = pr NA + a
+// (pr = 0: rho1, 1: rho2), chain c by issuer c mod XATU_PANEL_NISSUE, the issuers in different warps (different SM
+// sub-partitions) side by side.  The shared-memory descriptors of an issuer's chains are formed once, for stage 0,
+// in a small table: a tile adds its stage offset to the B descriptors, each further K step of an atom 256 bytes to
+// both.  One commit per issuer and tile to the tile's done barrier.
+template <int NV, int NC, int NA>
 __device__ __forceinline__ void panel_mma(const AsmPanelGeom& g, unsigned char* smem, uint64_t* full, uint64_t* done,
                                           uint64_t* afull, uint64_t* tfree, uint64_t* desc, uint32_t tmem, int t0,
-                                          int nt, int* status, volatile int* abort) {
+                                          int nt, int issuer, int* status, volatile int* abort) {
   using S = PanelShape<NV, NC, NA>;
-  constexpr int NBS = XATU_PANEL_NBS, NSLOT = S::NSLOT, ND = XATU_PANEL_NDONE;
+  constexpr int NBS = XATU_PANEL_NBS, NSLOT = S::NSLOT, ND = XATU_PANEL_NDONE, NI = XATU_PANEL_NISSUE;
+  constexpr int NCH = (2 * NA + NI - 1) / NI;   // chains per issuer (at most)
   static_assert(ND % NSLOT == 0, "done ring");
-  constexpr uint32_t id = asm_idesc_f16(PR == 0 ? S::N1 : S::N2);
-  // desc[4 a + {0, 1, 2, 3}] = A hi, A lo, B hi, B lo (stage 0); desc[4 NA + a] = K steps
+  // desc[5 x + {0, 1, 2, 3}] = A hi, A lo, B hi, B lo (stage 0) of the issuer's chain x, desc[5 x + 4] = K steps
 #pragma unroll
-  for (int a = 0; a < NA; a++) {
+  for (int x = 0; x < NCH; x++) {
+    const int c = issuer + x * NI;
+    if (c >= 2 * NA) break;
+    const int pr = c / NA, a = c - pr * NA;
     const int Ka = g.koff[a + 1] - g.koff[a];
-    const unsigned char* A = smem + (size_t)PR * 2 * g.a_plane + (uint32_t)(g.koff[a] / 8) * 128;
-    const unsigned char* B = smem + g.s_B + g.b_off[PR][a];
-    uint64_t* d = desc + 4 * a;
+    const unsigned char* A = smem + (size_t)pr * 2 * g.a_plane + (uint32_t)(g.koff[a] / 8) * 128;
+    const unsigned char* B = smem + g.s_B + g.b_off[pr][a];
+    uint64_t* d = desc + 5 * x;
     d[0] = asm_desc_noswz(A, g.KPT * 16);
     d[1] = asm_desc_noswz(A + g.a_plane, g.KPT * 16);
     d[2] = asm_desc_noswz(B, Ka * 16);
-    d[3] = asm_desc_noswz(B + g.b_plane[PR][a], Ka * 16);
-    desc[4 * NA + a] = (uint64_t)(Ka / 16);
+    d[3] = asm_desc_noswz(B + g.b_plane[pr][a], Ka * 16);
+    d[4] = (uint64_t)(Ka / 16);
   }
   PanelIter it = panel_locate<S>(t0, g.npanel, g.ntile);
   int cur = -1, nA = 0, last = -1;
@@ -451,14 +456,18 @@ __device__ __forceinline__ void panel_mma(const AsmPanelGeom& g, unsigned char* 
     if (!(ok = panel_wait(&full[st], (t / NBS) & 1, abort))) break;
     if (t >= NSLOT && !(ok = panel_wait(&tfree[slot], ((t / NSLOT) - 1) & 1, abort))) break;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t dbase = tmem + (uint32_t)(slot * S::SLOT_STRIDE) + (PR == 0 ? 0 : NA * S::N1);
+    const uint32_t dbase = tmem + (uint32_t)(slot * S::SLOT_STRIDE);
     const uint64_t boff = (uint64_t)((st * g.b_bytes) >> 4);
 #pragma unroll
-    for (int a = 0; a < NA; a++) {
-      const uint64_t* d4 = desc + 4 * a;
-      const uint64_t ah = d4[0], al = d4[1], bh = d4[2] + boff, bl = d4[3] + boff;
-      const int steps = (int)desc[4 * NA + a];
-      const uint32_t dcol = dbase + a * (PR == 0 ? S::N1 : S::N2);
+    for (int x = 0; x < NCH; x++) {
+      const int c = issuer + x * NI;
+      if (c >= 2 * NA) break;
+      const int pr = c / NA, a = c - pr * NA;
+      const uint64_t* d5 = desc + 5 * x;
+      const uint64_t ah = d5[0], al = d5[1], bh = d5[2] + boff, bl = d5[3] + boff;
+      const int steps = (int)d5[4];
+      const uint32_t dcol = dbase + (pr == 0 ? a * S::N1 : NA * S::N1 + a * S::N2);
+      const uint32_t id = pr == 0 ? asm_idesc_f16(S::N1) : asm_idesc_f16(S::N2);
       for (int k = 0; k < steps; k++) {
         const uint64_t o = (uint64_t)(16 * k);   // 256 bytes along K
         asm_umma(dcol, ah + o, bh + o, id, k > 0 ? 1u : 0u);
@@ -474,7 +483,7 @@ __device__ __forceinline__ void panel_mma(const AsmPanelGeom& g, unsigned char* 
     *abort = 1;
   }
   // products in flight complete before the CTA's shared and tensor memory are released (the commit tracks this
-  // thread's products; the barrier's phase also needs the other product thread's, so the wait is bounded)
+  // thread's products; the barrier's phase also needs the other issuers', so the wait is bounded)
   if (last >= 0) asm_mbar_wait(&done[last % ND], (last / ND) & 1);
 }
 
@@ -845,7 +854,7 @@ bse_assemble_panel_kernel(AsmParams p, AsmInputs in, AsmOutputs out, AsmPanelGeo
   constexpr int NBS = XATU_PANEL_NBS;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint64_t s_full[NBS], s_done[XATU_PANEL_NDONE], s_afull, s_tfree[2];
-  __shared__ uint64_t s_desc[2][5 * NA];
+  __shared__ uint64_t s_desc[XATU_PANEL_NISSUE][5 * ((2 * NA + XATU_PANEL_NISSUE - 1) / XATU_PANEL_NISSUE)];
   __shared__ uint32_t s_tmem;
   __shared__ int s_abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -860,8 +869,8 @@ bse_assemble_panel_kernel(AsmParams p, AsmInputs in, AsmOutputs out, AsmPanelGeo
   if (tid == 0) {
     for (int st = 0; st < NBS; st++)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_full[st])), "r"(1));
-    for (int d = 0; d < XATU_PANEL_NDONE; d++)   // one commit from each of the two product threads
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_done[d])), "r"(2));
+    for (int d = 0; d < XATU_PANEL_NDONE; d++)   // one commit from each product thread
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_done[d])), "r"(XATU_PANEL_NISSUE));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_afull)), "r"(1));
     for (int s = 0; s < 2; s++)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(asm_smem_u32(&s_tfree[s])), "r"(XATU_PANEL_NCW));
@@ -878,10 +887,10 @@ bse_assemble_panel_kernel(AsmParams p, AsmInputs in, AsmOutputs out, AsmPanelGeo
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(XATU_PANEL_REGS_PRODUCER));
     if (warp == XATU_PANEL_NCW && lane == 0 && nt > 0)
       panel_copier<NV, NC, NA>(g, in.tc_ops, smem, s_full, s_done, &s_afull, t0, nt, in.status, abort);
-    if (warp == XATU_PANEL_NCW + 1 && lane == 0 && nt > 0)
-      panel_mma<NV, NC, NA, 0>(g, smem, s_full, s_done, &s_afull, s_tfree, s_desc[0], tmem, t0, nt, in.status, abort);
-    if (warp == XATU_PANEL_NCW + 2 && lane == 0 && nt > 0)
-      panel_mma<NV, NC, NA, 1>(g, smem, s_full, s_done, &s_afull, s_tfree, s_desc[1], tmem, t0, nt, in.status, abort);
+    const int issuer = warp - XATU_PANEL_NCW - 1;
+    if (issuer >= 0 && issuer < XATU_PANEL_NISSUE && lane == 0 && nt > 0)
+      panel_mma<NV, NC, NA>(g, smem, s_full, s_done, &s_afull, s_tfree, s_desc[issuer], tmem, t0, nt, issuer,
+                            in.status, abort);
   } else {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(XATU_PANEL_REGS_CONSUMER));
     panel_consumer<NV, NC, NA>(p, in, out, g, smem, s_done, s_tfree, tmem, t0, nt, warp, lane, abort);
