@@ -670,22 +670,26 @@ __device__ __forceinline__ void panel_consumer(const AsmParams& p, const AsmInpu
     const uint32_t cbase = tl + (uint32_t)(slot * S::SLOT_STRIDE);
     const int kp0 = it.j * TKC + 2 * cg;
     int en[2] = {0, 0};
+    // overlaps of both k' points of the warp, then the slot is free for the products of a later tile
+    float r2q[2][NA][2 * NV], r1q[2][NA][2 * NC];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int kq = 2 * cg + q;
+#pragma unroll
+      for (int b = 0; b < NA; b++) panel_tmem_ld<2 * NV>(cbase + NA * S::N1 + b * S::N2 + kq * 2 * NV, r2q[q][b]);
+#pragma unroll
+      for (int a = 0; a < NA; a++) panel_tmem_ld<2 * NC>(cbase + a * S::N1 + kq * 2 * NC, r1q[q][a]);
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(asm_smem_u32(&tfree[slot])) : "memory");
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const int kq = 2 * cg + q;   // k' of the tile
       const int kp = kp0 + q;
-      float r2[NA][2 * NV], r1[NA][2 * NC];
-#pragma unroll
-      for (int b = 0; b < NA; b++) panel_tmem_ld<2 * NV>(cbase + NA * S::N1 + b * S::N2 + kq * 2 * NV, r2[b]);
-#pragma unroll
-      for (int a = 0; a < NA; a++) panel_tmem_ld<2 * NC>(cbase + a * S::N1 + kq * 2 * NC, r1[a]);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (q == 1) {
-        // the slot is free for the products of a later tile
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(asm_smem_u32(&tfree[slot])) : "memory");
-      }
+      float (&r2)[NA][2 * NV] = r2q[q];
+      float (&r1)[NA][2 * NC] = r1q[q];
       // T_a(v', beta) = sum_b (-V_ab) rho2_b(v', beta), V_ba = conj(V_ab)
       float2 T[NA][NV];
 #pragma unroll
