@@ -23,8 +23,9 @@
 // Kernel structure (one CTA per SM, persistent): the tiles of the upper block triangle, enumerated row block
 // by row block, are cut into equal contiguous ranges, one per CTA.
 //   * warp 0: TMA producer, an XHH_STAGES-deep ring of stages (A_hi, A_lo, Bt_hi, Bt_lo, Bu_hi, Bu_lo);
-//   * warp 1: one thread issues tcgen05.mma (M = 128, N = ng, K = 16).  The direct accumulator of a row block
-//     (a segment of the range) takes a slot of a ring of two in tensor memory, the transposed accumulator of a
+//   * warps 1 and 2: one thread each issues tcgen05.mma (M = 128, N = ng, K = 16), warp 1 the direct products,
+//     warp 2 the transposed ones; a ring stage is free once both have committed it.  The direct accumulator of a
+//     row block (a segment of the range) takes a slot of a ring of two in tensor memory, the transposed accumulator of a
 //     tile one of a ring of XHH_TSLOTS; tcgen05.commit frees ring stages and publishes finished accumulators;
 //   * warps 4-7: epilogue, tcgen05.ld of the accumulator lanes, FP32 vector atomics into Y (row-major N x ng),
 //     then an arrive that frees the accumulator slot;
@@ -205,7 +206,7 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
   if (threadIdx.x == 0) {
     for (int s = 0; s < XHH_STAGES; s++) {
       mbar_init(&sh->full[s], 1);
-      mbar_init(&sh->empty[s], 1);
+      mbar_init(&sh->empty[s], 2);   // one commit from each MMA issuer
     }
     for (int a = 0; a < 2; a++) {
       mbar_init(&sh->dfull[a], 1);
@@ -215,7 +216,7 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
       mbar_init(&sh->tfull[a], 1);
       mbar_init(&sh->tempty[a], 4);
     }
-    mbar_init(&sh->drain, 1);
+    mbar_init(&sh->drain, 2);
     sh->abort_flag = 0;
     sh->issued = 0;
     sh->consumed = 0;
@@ -269,9 +270,11 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
         sh->issued = li + 1;
       }
     }
-  } else if (warp == 1) {
+  } else if (warp == 1 || warp == 2) {
     if (lane == 0 && t1 > t0) {
-      // ---------------- MMA issuer
+      // ---------------- MMA issuers: warp 1 the direct products, warp 2 the transposed ones (two threads on different
+      // SM sub-partitions issue side by side; a ring stage is free once both have committed it)
+      const bool direct = warp == 1;
       constexpr uint32_t idesc_d = umma_idesc_bf16(NG, 0);
       constexpr uint32_t idesc_t = umma_idesc_bf16(NG, 1);
       int I, t;
@@ -289,61 +292,65 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        if (I != curI) {   // a new row block: the next direct slot, once the epilogue has emptied it
-          seg++;
-          curI = I;
-          dslot = (uint32_t)(seg & 1);
-          if (seg >= 2 && !mbar_wait(&sh->dempty[dslot], (uint32_t)(((seg >> 1) - 1) & 1), abort_flag)) {
-            atomicOr(p.status, XATU_DEVERR_NOCONV);
-            *abort_flag = 1;
-            break;
-          }
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          dfresh = true;
-        }
         const bool diag = (t >> 1) == I;
         const unsigned char* st = ring + s * STAGE;
-        const uint32_t dtm = tmem + dslot * NG;
-#pragma unroll
-        for (int kk = 0; kk < 2 * XHH_BOX / 16; kk++) {
-          const uint32_t ao = (kk >> 2) * A_BOX + (kk & 3) * 32, bo = (kk >> 2) * B_BOX + (kk & 3) * 32;
-          const uint64_t ahi = umma_desc_sw128(st + ao, 0), alo = umma_desc_sw128(st + A_PLANE + ao, 0);
-          const uint64_t bhi = umma_desc_sw128(st + OFF_BT + bo, 0);
-          const uint64_t blo = umma_desc_sw128(st + OFF_BT + B_PLANE + bo, 0);
-          umma_bf16(dtm, ahi, bhi, idesc_d, (dfresh && kk == 0) ? 0u : 1u);
-          umma_bf16(dtm, ahi, blo, idesc_d, 1u);
-          umma_bf16(dtm, alo, bhi, idesc_d, 1u);
-        }
-        dfresh = false;
-        if (!diag) {
-          const uint32_t tslot = (uint32_t)(tcount % XHH_TSLOTS);
-          const int tuse = tcount / XHH_TSLOTS;
-          if (tuse >= 1 && !mbar_wait(&sh->tempty[tslot], (uint32_t)((tuse - 1) & 1), abort_flag)) {
-            atomicOr(p.status, XATU_DEVERR_NOCONV);
-            *abort_flag = 1;
-            break;
+        if (direct) {
+          if (I != curI) {   // a new row block: the next direct slot, once the epilogue has emptied it
+            seg++;
+            curI = I;
+            dslot = (uint32_t)(seg & 1);
+            if (seg >= 2 && !mbar_wait(&sh->dempty[dslot], (uint32_t)(((seg >> 1) - 1) & 1), abort_flag)) {
+              atomicOr(p.status, XATU_DEVERR_NOCONV);
+              *abort_flag = 1;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            dfresh = true;
           }
-          asm volatile("tcgen05.fence::after_thread_sync;");
-          const uint32_t ttm = tmem + (2 + tslot) * NG;
+          const uint32_t dtm = tmem + dslot * NG;
 #pragma unroll
-          for (int kk = 0; kk < XHH_BM / 16; kk++) {
-            // K step: 16 rows of the tile = two 8-row groups (2048 B); M: the two 64-column boxes, A_BOX apart
-            const uint32_t ao = kk * 2048, bo = (kk >> 2) * B_BOX + (kk & 3) * 32;
-            const uint64_t ahi = umma_desc_sw128(st + ao, A_BOX), alo = umma_desc_sw128(st + A_PLANE + ao, A_BOX);
-            const uint64_t uhi = umma_desc_sw128(st + OFF_BU + bo, 0);
-            const uint64_t ulo = umma_desc_sw128(st + OFF_BU + B_PLANE + bo, 0);
-            umma_bf16(ttm, ahi, uhi, idesc_t, kk == 0 ? 0u : 1u);
-            umma_bf16(ttm, ahi, ulo, idesc_t, 1u);
-            umma_bf16(ttm, alo, uhi, idesc_t, 1u);
+          for (int kk = 0; kk < 2 * XHH_BOX / 16; kk++) {
+            const uint32_t ao = (kk >> 2) * A_BOX + (kk & 3) * 32, bo = (kk >> 2) * B_BOX + (kk & 3) * 32;
+            const uint64_t ahi = umma_desc_sw128(st + ao, 0), alo = umma_desc_sw128(st + A_PLANE + ao, 0);
+            const uint64_t bhi = umma_desc_sw128(st + OFF_BT + bo, 0);
+            const uint64_t blo = umma_desc_sw128(st + OFF_BT + B_PLANE + bo, 0);
+            umma_bf16(dtm, ahi, bhi, idesc_d, (dfresh && kk == 0) ? 0u : 1u);
+            umma_bf16(dtm, ahi, blo, idesc_d, 1u);
+            umma_bf16(dtm, alo, bhi, idesc_d, 1u);
           }
-          umma_commit(&sh->tfull[tslot]);
-          tcount++;
+          dfresh = false;
+          sh->consumed = li + 1;
+          umma_commit(&sh->empty[s]);           // ring stage free once both issuers' MMAs complete
+          if (t + 1 == p.nt || g + 1 == t1) umma_commit(&sh->dfull[dslot]);
+        } else {
+          if (!diag) {
+            const uint32_t tslot = (uint32_t)(tcount % XHH_TSLOTS);
+            const int tuse = tcount / XHH_TSLOTS;
+            if (tuse >= 1 && !mbar_wait(&sh->tempty[tslot], (uint32_t)((tuse - 1) & 1), abort_flag)) {
+              atomicOr(p.status, XATU_DEVERR_NOCONV);
+              *abort_flag = 1;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t ttm = tmem + (2 + tslot) * NG;
+#pragma unroll
+            for (int kk = 0; kk < XHH_BM / 16; kk++) {
+              // K step: 16 rows of the tile = two 8-row groups (2048 B); M: the two 64-column boxes, A_BOX apart
+              const uint32_t ao = kk * 2048, bo = (kk >> 2) * B_BOX + (kk & 3) * 32;
+              const uint64_t ahi = umma_desc_sw128(st + ao, A_BOX), alo = umma_desc_sw128(st + A_PLANE + ao, A_BOX);
+              const uint64_t uhi = umma_desc_sw128(st + OFF_BU + bo, 0);
+              const uint64_t ulo = umma_desc_sw128(st + OFF_BU + B_PLANE + bo, 0);
+              umma_bf16(ttm, ahi, uhi, idesc_t, kk == 0 ? 0u : 1u);
+              umma_bf16(ttm, ahi, ulo, idesc_t, 1u);
+              umma_bf16(ttm, alo, uhi, idesc_t, 1u);
+            }
+            umma_commit(&sh->tfull[tslot]);
+            tcount++;
+          }
+          umma_commit(&sh->empty[s]);
         }
-        sh->consumed = li + 1;
-        umma_commit(&sh->empty[s]);           // ring stage free once these MMAs complete
-        if (t + 1 == p.nt || g + 1 == t1) umma_commit(&sh->dfull[dslot]);
       }
-      // drain: every MMA issued so far has completed once this commit arrives
+      // drain: every MMA either issuer issued has completed once both commits arrive
       umma_commit(&sh->drain);
       mbar_wait(&sh->drain, 0, nullptr);
     }
