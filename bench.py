@@ -676,7 +676,10 @@ def run_engine(args):
     n_stored = stored_kernel_elements(N)
     asm_s = statistics.median(asm_ms) / 1e3
     asm_bytes = n_stored * 8 + N * 8
-    kernels = [{"kernel": "bse_assemble_tile_kernel<float,2,2,3,mixed>", "bound": "hbm",
+    asm_path = ex.kernelStats("assembly")[2]
+    asm_name = {3: "bse_assemble_panel_kernel<2,2,3> (with its operand formatting and diagonal-block mirror)",
+                2: "bse_assemble_tile_tc_kernel<2,2,3,16>", 0: "bse_assemble_tile_kernel<float,2,2,3,mixed>"}
+    kernels = [{"kernel": asm_name.get(asm_path, "assembly path %d" % asm_path), "bound": "hbm",
                 "achieved": asm_bytes / asm_s / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": asm_bytes / asm_s / 1e9 / hbm, "peak_source": src, "traffic": None,
                 "algorithmic_bytes_per_launch": asm_bytes, "launch_ms": asm_s * 1e3, "launches_per_step": 1}]
