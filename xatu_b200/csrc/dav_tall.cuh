@@ -65,29 +65,32 @@ ts_proj_kernel(const cd* __restrict__ A, int a, const cd* __restrict__ B, int b,
 }
 
 // Z[r + c * ldz] = sum_g part[g][r + c * a] for o = r + c * a < n, the tiles g added in order.  One CTA per
-// 32 outputs: 8 threads per output over strided g (eight loads in flight each), then a fixed-order sum.
+// 32 outputs per CTA of TS_SUM_THREADS: the 32 warps split the tiles g (warp w takes g = w, w + 32, ...; every
+// load of a thread is in flight at once), then a fixed-order sum over the warps (deterministic).
 // status_out (may be NULL) receives a copy of the device status word, for a single read-back.
-__global__ void __launch_bounds__(TS_THREADS)
+#define TS_SUM_THREADS 1024
+__global__ void __launch_bounds__(TS_SUM_THREADS)
 ts_sum_kernel(const cd* __restrict__ part, int G, int n, int a, cd* __restrict__ Z, int ldz,
               const int* __restrict__ status_in, double* __restrict__ status_out) {
-  __shared__ double red[8][32][2];
+  constexpr int NWS = TS_SUM_THREADS / 32;
+  __shared__ double red[NWS][32][2];
   if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *status_out = (double)*status_in;
   const int ol = threadIdx.x & 31, gl = threadIdx.x >> 5;
   const int o = blockIdx.x * 32 + ol;
   double sx = 0.0, sy = 0.0;
   if (o < n) {
     int g = gl;
-    for (; g + 56 < G; g += 64) {
+    for (; g + 7 * NWS < G; g += 8 * NWS) {
       double2 p[8];
 #pragma unroll
-      for (int u = 0; u < 8; u++) p[u] = __ldcg(reinterpret_cast<const double2*>(part + (size_t)(g + 8 * u) * n + o));
+      for (int u = 0; u < 8; u++) p[u] = __ldcg(reinterpret_cast<const double2*>(part + (size_t)(g + NWS * u) * n + o));
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         sx += p[u].x;
         sy += p[u].y;
       }
     }
-    for (; g < G; g += 8) {
+    for (; g < G; g += NWS) {
       const double2 p = __ldcg(reinterpret_cast<const double2*>(part + (size_t)g * n + o));
       sx += p.x;
       sy += p.y;
@@ -98,8 +101,8 @@ ts_sum_kernel(const cd* __restrict__ part, int G, int n, int a, cd* __restrict__
   __syncthreads();
   if (gl == 0 && o < n) {
     double tx = 0.0, ty = 0.0;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
+#pragma unroll 8
+    for (int q = 0; q < NWS; q++) {
       tx += red[q][ol][0];
       ty += red[q][ol][1];
     }

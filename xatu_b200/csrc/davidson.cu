@@ -287,7 +287,7 @@ static xatu_status ts_proj(xatu_ctx* ctx, const cd* A, int a, const cd* B, int b
   ts_proj_kernel<<<G, TS_THREADS, ts_proj_smem(a, b, TR), ctx->stream>>>(A, a, B, b, N, TR, ctx->dv_part.as<cd>());
   ctx->launches++;
   XATU_CK_LAUNCH("ts_proj_kernel");
-  ts_sum_kernel<<<(ab + 31) / 32, TS_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, ab, a, Z, ldz,
+  ts_sum_kernel<<<(ab + 31) / 32, TS_SUM_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, ab, a, Z, ldz,
                                                                  ctx->d_status.as<int>(), status_out);
   ctx->launches++;
   XATU_CK_LAUNCH("ts_sum_kernel");
@@ -469,7 +469,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
       ctx->launches++;
       XATU_CK_LAUNCH("ts_ritz_kernel");
       // squared residual norms as complex pairs at [256, 256 + 2 nritz), the status word at 768
-      ts_sum_kernel<<<(nritz + 31) / 32, TS_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, nritz, nritz,
+      ts_sum_kernel<<<(nritz + 31) / 32, TS_SUM_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, nritz, nritz,
                                                                          reinterpret_cast<cd*>(norms), 1,
                                                                          ctx->d_status.as<int>(), theta + 768);
       ctx->launches++;
