@@ -21,7 +21,6 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
-#include <numeric>
 #include <vector>
 
 #include "engine.h"
@@ -56,6 +55,83 @@ __device__ __forceinline__ double dav_noise(unsigned long long i, unsigned long 
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   z ^= z >> 31;
   return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// The nsel lowest entries of d, ties resolved by the lower index, in ascending order into idx (the start
+// columns of the Davidson basis), and *kept = nsel.  One CTA: every thread keeps the lowest untaken entry of its
+// strided share; each round a block-wide arg-min picks the winner, whose owner marks it taken in the scratch copy
+// w and rescans its share.
+#define DAV_SEL_THREADS 1024
+__device__ __forceinline__ bool dav_sel_less(double a, long long ia, double b, long long ib) {
+  return a < b || (a == b && ia < ib);
+}
+__global__ void __launch_bounds__(DAV_SEL_THREADS)
+dav_select_lowest_kernel(const double* __restrict__ d, long long N, int nsel, double* __restrict__ w,
+                         int* __restrict__ idx, int* __restrict__ kept) {
+  __shared__ double sv[DAV_SEL_THREADS / 32];
+  __shared__ long long si[DAV_SEL_THREADS / 32];
+  __shared__ long long win;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double best = INFINITY;
+  long long bi = N;
+  for (long long i = tid; i < N; i += DAV_SEL_THREADS) {
+    const double v = d[i];
+    w[i] = v;
+    if (dav_sel_less(v, i, best, bi)) {
+      best = v;
+      bi = i;
+    }
+  }
+  for (int r = 0; r < nsel; r++) {
+    double b = best;
+    long long ib = bi;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, b, o);
+      const long long oi = __shfl_xor_sync(0xffffffffu, ib, o);
+      if (dav_sel_less(ob, oi, b, ib)) {
+        b = ob;
+        ib = oi;
+      }
+    }
+    if (lane == 0) {
+      sv[warp] = b;
+      si[warp] = ib;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      b = lane < DAV_SEL_THREADS / 32 ? sv[lane] : INFINITY;
+      ib = lane < DAV_SEL_THREADS / 32 ? si[lane] : N;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, b, o);
+        const long long oi = __shfl_xor_sync(0xffffffffu, ib, o);
+        if (dav_sel_less(ob, oi, b, ib)) {
+          b = ob;
+          ib = oi;
+        }
+      }
+      if (lane == 0) {
+        win = ib;
+        idx[r] = (int)(ib < N ? ib : r);   // fewer than nsel finite entries: any column
+      }
+    }
+    __syncthreads();
+    const long long wi = win;
+    if (wi < N && wi % DAV_SEL_THREADS == tid) {
+      w[wi] = INFINITY;
+      best = INFINITY;
+      bi = N;
+      for (long long i = tid; i < N; i += DAV_SEL_THREADS) {
+        const double v = w[i];
+        if (dav_sel_less(v, i, best, bi)) {
+          best = v;
+          bi = i;
+        }
+      }
+    }
+  }
+  if (tid == 0) *kept = nsel;
 }
 
 __global__ void dav_start_vectors_kernel(cd* V, long long N, int col0, const int* idx, int nvec, double noise) {
@@ -393,15 +469,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     ctx->launches++;
     XATU_CK(cudaGetLastError());
   }
-  std::vector<double> hdiag(N);
-  XATU_CK(cudaMemcpyAsync(hdiag.data(), diagH, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  XATU_CK(cudaStreamSynchronize(ctx->stream));
-  std::vector<int> order(N);
-  std::iota(order.begin(), order.end(), 0);
-  std::partial_sort(order.begin(), order.begin() + bsz, order.end(),
-                    [&](int a, int b) { return hdiag[a] < hdiag[b] || (hdiag[a] == hdiag[b] && a < b); });
-  XATU_CK(cudaMemcpyAsync(sel_dev, order.data(), bsz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-  XATU_CK(cudaMemcpyAsync(dkept, &bsz, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  // start columns: the bsz lowest diagonal entries, chosen on the device (no host round trip)
+  dav_select_lowest_kernel<<<1, DAV_SEL_THREADS, 0, ctx->stream>>>(diagH, N, bsz,
+                                                                   reinterpret_cast<double*>(ctx->dv_tmp.p), sel_dev,
+                                                                   dkept);
+  ctx->launches++;
+  XATU_CK(cudaGetLastError());
   {
     // unit vectors of the lowest diagonal entries plus noise of norm ~1e-3 per column, orthonormalised below
     // (enough to seed every symmetry sector; larger noise costs Davidson steps to remove again)
