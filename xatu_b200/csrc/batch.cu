@@ -9,11 +9,13 @@
 //     device work list of (system, tile) items taken through an atomic
 //     counter, largest systems first; the tile size of each class is chosen by
 //     the autotuner (timed candidates on the batch's own data, first run);
-//   * the iteration graph: one step of a block Davidson run in lockstep for all
-//     systems, with every decision taken on the device (Rayleigh-Ritz, restart,
-//     convergence, orthonormalisation), so the host only replays the graph and
-//     reads the number of systems still active.  Converged systems skip their
-//     work, the tcgen05 K.X product included.
+//   * the solve graph: a conditional WHILE node whose body is one step of a
+//     block Davidson run in lockstep for all systems, with every decision taken
+//     on the device (Rayleigh-Ritz, restart, convergence, orthonormalisation);
+//     a one-thread kernel at the end of the body counts the step and sets the
+//     loop condition (systems still active, iteration cap), so the whole solve
+//     is one graph launch with no host round trip per step.  Converged systems
+//     skip their work, the tcgen05 K.X product included.
 //
 // Davidson step of one system (basis V, W = H V, projected matrix T = V^H W
 // grown by the new columns only; block P of at most BD_MAXB new directions):
@@ -560,6 +562,14 @@ __global__ void bd_count_kernel(BDGlobal g, const BDav* D, int* count) {
   if (threadIdx.x == 0) *count = c;
 }
 
+// Loop control of the solve graph (body of its conditional WHILE node): counts the finished lockstep iteration
+// and keeps the loop running while a member is still active and the iteration cap is not reached.
+__global__ void bd_loop_kernel(cudaGraphConditionalHandle h, const int* __restrict__ count, int* __restrict__ iters,
+                               int max_iter) {
+  const int it = ++*iters;
+  cudaGraphSetConditional(h, (*count > 0 && it < max_iter) ? 1u : 0u);
+}
+
 // ------------------------------------------------------------------ host side
 struct BatchClass {
   int nv, nc, na, tk;
@@ -583,7 +593,7 @@ struct xatu_batch {
   BDGlobal g{};
   BDGlobal chosen{};
   std::vector<BDav> hdesc;
-  DBuf d_desc, d_row_off, d_red_off, d_count, d_status, d_arena;
+  DBuf d_desc, d_row_off, d_red_off, d_count, d_iters, d_status, d_arena;
   int nrow = 0, nred = 0;
   int* h_count = nullptr;        // pinned
   cudaGraphExec_t build_exec = nullptr, iter_exec = nullptr;
@@ -727,8 +737,8 @@ static xatu_status enqueue_build(xatu_batch* b, bool with_assembly, bool with_in
 
 static size_t rr_smem() { return heev_smem_bytes(BD_MMAX, BD_MAXB); }
 
-// One Davidson step for every active member.
-static xatu_status enqueue_iteration(xatu_batch* b) {
+// One Davidson step for every active member; to_host: the number of active members is also copied to the host.
+static xatu_status enqueue_iteration(xatu_batch* b, bool to_host) {
   const BDGlobal g = b->g;
   BDav* D = b->d_desc.as<BDav>();
   const int* ro = b->d_row_off.as<int>();
@@ -762,38 +772,83 @@ static xatu_status enqueue_iteration(xatu_batch* b) {
   bd_apply_s_kernel<<<b->nrow, BD_ROWS, 0, b->stream>>>(g, D, ro);
   bd_count_kernel<<<1, 32, 0, b->stream>>>(g, D, b->d_count.as<int>());
   BCK(cudaGetLastError());
-  BCK(cudaMemcpyAsync(b->h_count, b->d_count.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  if (to_host) BCK(cudaMemcpyAsync(b->h_count, b->d_count.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   return XATU_OK;
 }
 
-// Build graph, then the iteration graph until no system is active; device ms of the whole solve.
-static xatu_status run_graphs(xatu_batch* b, cudaGraphExec_t build, cudaGraphExec_t iter, int* iters, float* ms) {
+// Build graph, then the solve graph (the lockstep iterations under a conditional WHILE node: the loop runs on the
+// device until no system is active or the iteration cap is reached, without a host round trip per iteration);
+// device ms of the whole solve.
+static xatu_status run_graphs(xatu_batch* b, cudaGraphExec_t build, cudaGraphExec_t solve, int* iters, float* ms) {
+  BCK(cudaMemsetAsync(b->d_iters.p, 0, sizeof(int), b->stream));
   BCK(cudaEventRecord(b->ev[0], b->stream));
   BCK(cudaGraphLaunch(build, b->stream));
   BCK(cudaEventRecord(b->ev[1], b->stream));
-  int it = 0;
-  for (; it < b->max_iter; it++) {
-    BCK(cudaGraphLaunch(iter, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    if (*b->h_count == 0) {
-      it++;
-      break;
-    }
-  }
+  BCK(cudaGraphLaunch(solve, b->stream));
   BCK(cudaEventRecord(b->ev[2], b->stream));
-  BCK(cudaEventSynchronize(b->ev[2]));
+  int h_it = 0;
+  BCK(cudaMemcpyAsync(b->h_count, b->d_count.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaMemcpyAsync(&h_it, b->d_iters.p, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
   cudaEventElapsedTime(&b->build_ms, b->ev[0], b->ev[1]);
   cudaEventElapsedTime(&b->solve_ms, b->ev[1], b->ev[2]);
-  b->iterations = it;
+  b->iterations = h_it;
   if (ms) *ms = b->build_ms + b->solve_ms;
-  if (iters) *iters = it;
+  if (iters) *iters = h_it;
+  return XATU_OK;
+}
+
+// The solve graph: one conditional WHILE node (condition set to 1 at every launch) whose body is one lockstep
+// iteration followed by bd_loop_kernel.
+static xatu_status capture_solve(xatu_batch* b, cudaGraphExec_t* exec) {
+  cudaGraph_t graph = nullptr;
+  BCK(cudaGraphCreate(&graph, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {};
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    BCK(e);
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    BCK(e);
+  }
+  xatu_status st = enqueue_iteration(b, false);
+  if (st == XATU_OK) {
+    bd_loop_kernel<<<1, 1, 0, b->stream>>>(h, b->d_count.as<int>(), b->d_iters.as<int>(), b->max_iter);
+    if ((e = cudaGetLastError()) != cudaSuccess) st = bfail(b, XATU_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(b->stream, &captured);
+  if (st != XATU_OK) {
+    cudaGraphDestroy(graph);
+    return st;
+  }
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    BCK(e);
+  }
+  e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  BCK(e);
   return XATU_OK;
 }
 
 static xatu_status capture(xatu_batch* b, bool build, cudaGraphExec_t* exec) {
   cudaGraph_t graph = nullptr;
   BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
-  xatu_status st = build ? enqueue_build(b, true, true) : enqueue_iteration(b);
+  xatu_status st = build ? enqueue_build(b, true, true) : enqueue_iteration(b, true);   // (the solve: capture_solve)
   cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
   if (st != XATU_OK) {
     if (graph) cudaGraphDestroy(graph);
@@ -944,6 +999,7 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
   BCK(cudaMemcpyAsync(b->d_row_off.p, ro.data(), ro.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   BCK(cudaMemcpyAsync(b->d_red_off.p, rd.data(), rd.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   BCK(b->d_count.ensure(sizeof(int)));
+  BCK(b->d_iters.ensure(sizeof(int)));
   BCK(b->d_status.ensure(sizeof(int)));
   BCK(cudaMemsetAsync(b->d_status.p, 0, sizeof(int), b->stream));
   if (!b->h_count) BCK(cudaMallocHost(&b->h_count, sizeof(int)));
@@ -960,7 +1016,7 @@ static xatu_status prepare(xatu_batch* b, int nstates, double tol) {
     b->g.mmax = basis_of(bs);
     cudaGraphExec_t be = nullptr, ie = nullptr;
     BTRY(capture(b, true, &be));
-    BTRY(capture(b, false, &ie));
+    BTRY(capture_solve(b, &ie));
     int it = 0;
     float ms = 0;
     const xatu_status st = run_graphs(b, be, ie, &it, &ms);
@@ -1021,7 +1077,7 @@ xatu_status xatu_batch_destroy(xatu_batch* b) {
     c.d_work.release();
     c.d_counter.release();
   }
-  for (DBuf* d : {&b->d_desc, &b->d_row_off, &b->d_red_off, &b->d_count, &b->d_status, &b->d_arena})
+  for (DBuf* d : {&b->d_desc, &b->d_row_off, &b->d_red_off, &b->d_count, &b->d_iters, &b->d_status, &b->d_arena})
     d->release();
   if (b->h_count) cudaFreeHost(b->h_count);
   for (xatu_ctx* c : b->members) xatu_ctx_destroy(c);
