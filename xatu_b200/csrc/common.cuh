@@ -14,6 +14,19 @@
 #define XATU_MAX_ORB 64
 #define XATU_MAX_BANDS 8   // per side (valence or conduction)
 
+// ------------------------------------------------ programmatic dependent launch
+// A kernel launched with programmatic stream serialisation (xatu_launch_chained) may start while its
+// predecessor on the stream is still running: xatu_grid_wait() returns once the predecessor grid has
+// completed and its writes are visible, so every kernel of such a chain calls it before its first access to
+// global memory.  xatu_grid_release() then lets the next kernel of the chain be scheduled (its blocks wait in
+// their own xatu_grid_wait()).  Outside a chained launch both are no-ops.
+__device__ __forceinline__ void xatu_grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void xatu_grid_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void xatu_grid_chain() {
+  xatu_grid_wait();
+  xatu_grid_release();
+}
+
 // ----------------------------------------------------------------- complex
 struct cd { double x, y; };
 struct cf { float x, y; };

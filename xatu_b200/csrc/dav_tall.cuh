@@ -4,7 +4,9 @@
 // staged into shared memory with 16-byte cp.async copies that are all in
 // flight at once (the blocks are L2-resident; the kernels are bound by load
 // latency, not bandwidth).  Reductions over the N rows are deterministic:
-// per-tile partial sums, then ts_sum_kernel adds them in tile order.
+// per-tile partial sums, then ts_sum_kernel adds them in tile order.  Every
+// kernel starts with xatu_grid_chain(), so that it can be launched chained to
+// its predecessor (xatu_launch_chained).
 #pragma once
 #include "common.cuh"
 
@@ -38,6 +40,7 @@ __host__ __device__ inline size_t ts_proj_smem(int a, int b, int TR) { return (s
 __global__ void __launch_bounds__(TS_THREADS)
 ts_proj_kernel(const cd* __restrict__ A, int a, const cd* __restrict__ B, int b, long long N, int TR,
                cd* __restrict__ part) {
+  xatu_grid_chain();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* sA = reinterpret_cast<cd*>(smem_raw);   // TR x (a + 1)
   cd* sB = sA + TR * (a + 1);                 // TR x (b + 1)
@@ -74,6 +77,7 @@ ts_sum_kernel(const cd* __restrict__ part, int G, int n, int a, cd* __restrict__
               const int* __restrict__ status_in, double* __restrict__ status_out) {
   constexpr int NWS = TS_SUM_THREADS / 32;
   __shared__ double red[NWS][32][2];
+  xatu_grid_chain();
   if (status_out && blockIdx.x == 0 && threadIdx.x == 0) *status_out = (double)*status_in;
   const int ol = threadIdx.x & 31, gl = threadIdx.x >> 5;
   const int o = blockIdx.x * 32 + ol;
@@ -115,6 +119,7 @@ ts_sum_kernel(const cd* __restrict__ part, int G, int n, int a, cd* __restrict__
 __global__ void __launch_bounds__(TS_THREADS)
 ts_update_kernel(const cd* In, int b, const cd* __restrict__ A, int a, const cd* __restrict__ C, int ldc,
                  const cd* __restrict__ S, cd* Out, long long N, int TR) {
+  xatu_grid_chain();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* sI = reinterpret_cast<cd*>(smem_raw);   // TR x (b + 1)
   cd* sO = sI + TR * (b + 1);                 // TR x (b + 1): In - A C
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(TS_THREADS)
 ts_ritz_kernel(const cd* __restrict__ V, const cd* __restrict__ W, int m, const cd* __restrict__ Y, int ldy, int k,
                const double* __restrict__ theta, const double* __restrict__ diagH, long long N, int TR,
                cd* __restrict__ U, cd* __restrict__ WU, cd* __restrict__ P, cd* __restrict__ part) {
+  xatu_grid_chain();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* sV = reinterpret_cast<cd*>(smem_raw);   // TR x (m + 1)
   cd* sW = sV + TR * (m + 1);                 // TR x (m + 1)
@@ -232,6 +238,7 @@ __host__ __device__ inline size_t ts_ritz_smem(int m, int k, int TR) {
 // Dst[:, j] = Src[:, sel[j]], j < nsel.
 __global__ void ts_gather_kernel(const cd* __restrict__ Src, const int* __restrict__ sel, int nsel, long long N,
                                  cd* __restrict__ Dst) {
+  xatu_grid_chain();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= N * nsel) return;
   const int j = (int)(t / N);
@@ -249,6 +256,7 @@ __global__ void ts_gather_kernel(const cd* __restrict__ Src, const int* __restri
 __global__ void __launch_bounds__(32)
 ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop, cd* __restrict__ S,
                     int* __restrict__ kept) {
+  xatu_grid_chain();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cd* A = reinterpret_cast<cd*>(smem_raw);        // b x b row-major, lower triangle -> L
   cd* M = A + b * b;                              // L_k^{-1}, row-major

@@ -29,6 +29,15 @@
 
 #define DAV_MAX_BASIS 112
 
+// Chained launch (xatu_launch_chained) on the context's stream, counted and checked.
+#define XATU_CHAIN(kernel, grid, block, smem, ...)                                                        \
+  do {                                                                                                   \
+    const cudaError_t e__ = xatu_launch_chained(kernel, dim3(grid), dim3(block), (size_t)(smem), ctx->stream, \
+                                                __VA_ARGS__);                                            \
+    ctx->launches++;                                                                                     \
+    if (e__ != cudaSuccess) return xatu_cuda_fail(ctx, e__, "launch of " #kernel);                      \
+  } while (0)
+
 // ---------------------------------------------------------------- kernels
 __global__ void dav_diag_mixed_kernel(const __nv_bfloat162* __restrict__ Khi, const __nv_bfloat162* __restrict__ Klo,
                                       const double* __restrict__ d, long long N, long long ldk, double* __restrict__ out) {
@@ -171,6 +180,7 @@ __global__ void dav_finish_w_kernel(const float2* __restrict__ Y, const double* 
 // the kept part, so they stay decoupled and never enter the lowest Ritz pairs (their Ritz coefficients
 // multiply zero columns).  The kept count is copied next to the Ritz values for the host's read-back.
 __global__ void dav_dead_kernel(cd* T, int ld, int m, int m0, const int* __restrict__ kept, double* kept_out) {
+  xatu_grid_chain();
   const int nnew = m - m0;
   const int kc = min(max(*kept, 0), nnew);
   if (threadIdx.x == 0) *kept_out = (double)kc;
@@ -199,6 +209,7 @@ __global__ void dav_dead_kernel(cd* T, int ld, int m, int m0, const int* __restr
 }
 
 __global__ void dav_hermitize_kernel(cd* T, int ld, int m, int m0) {
+  xatu_grid_chain();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int nnew = m - m0;
   if (t >= nnew * m) return;
@@ -219,6 +230,7 @@ __global__ void dav_hermitize_kernel(cd* T, int ld, int m, int m0) {
 
 // T = diag(theta[0:k])
 __global__ void dav_set_diag_kernel(cd* T, int ld, int k, const double* theta) {
+  xatu_grid_chain();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= k * k) return;
   const int r = t % k, c = t / k;
@@ -230,6 +242,7 @@ __global__ void __launch_bounds__(HEEV_THREADS)
 dav_heev_kernel(const cd* __restrict__ T, int ldt, int m, int k, double* __restrict__ theta, cd* __restrict__ Y,
                 int ldy, cd* __restrict__ refl, int* __restrict__ status, long long* __restrict__ prof) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  xatu_grid_chain();
   heev_lowest(T, ldt, m, k, theta, Y, ldy, refl, smem_raw, status, prof);
 }
 
@@ -240,6 +253,7 @@ dav_heev_kernel(const cd* __restrict__ T, int ldt, int m, int k, double* __restr
 __global__ void dav_finish_w_tc_kernel(const float* __restrict__ Y, const double* __restrict__ d,
                                        const cd* __restrict__ V, long long N, int col0, int b, int bp,
                                        cd* __restrict__ W) {
+  xatu_grid_chain();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= N * b) return;
   const int s = (int)(t / N);
@@ -293,10 +307,8 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv) {
       ctx->hx_last_path = 2;
       ctx->launches++;
       const long long tw = N * b;
-      dav_finish_w_tc_kernel<<<(int)((tw + threads - 1) / threads), threads, 0, ctx->stream>>>(
-          ctx->dv_Yf.as<float>(), ctx->d_diag.as<double>(), V, N, col0 + c, b, bp, W);
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
+      XATU_CHAIN(dav_finish_w_tc_kernel, (int)((tw + threads - 1) / threads), threads, 0, ctx->dv_Yf.as<float>(),
+                 ctx->d_diag.as<double>(), V, N, col0 + c, b, bp, W);
     }
     return XATU_OK;
   }
@@ -360,13 +372,9 @@ static xatu_status ts_proj(xatu_ctx* ctx, const cd* A, int a, const cd* B, int b
   const int G = (int)((N + TR - 1) / TR);
   const int ab = a * b;
   XATU_TRY(ts_part_ensure(ctx, (size_t)G * ab * sizeof(cd)));
-  ts_proj_kernel<<<G, TS_THREADS, ts_proj_smem(a, b, TR), ctx->stream>>>(A, a, B, b, N, TR, ctx->dv_part.as<cd>());
-  ctx->launches++;
-  XATU_CK_LAUNCH("ts_proj_kernel");
-  ts_sum_kernel<<<(ab + 31) / 32, TS_SUM_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, ab, a, Z, ldz,
-                                                                 ctx->d_status.as<int>(), status_out);
-  ctx->launches++;
-  XATU_CK_LAUNCH("ts_sum_kernel");
+  XATU_CHAIN(ts_proj_kernel, G, TS_THREADS, ts_proj_smem(a, b, TR), A, a, B, b, N, TR, ctx->dv_part.as<cd>());
+  XATU_CHAIN(ts_sum_kernel, (ab + 31) / 32, TS_SUM_THREADS, 0, ctx->dv_part.as<cd>(), G, ab, a, Z, ldz,
+             ctx->d_status.as<int>(), status_out);
   return XATU_OK;
 }
 
@@ -375,9 +383,7 @@ static xatu_status ts_update(xatu_ctx* ctx, const cd* In, int b, const cd* A, in
                              const cd* S, cd* Out, long long N) {
   const int TR = ts_pick_tile([&](int tr) { return ts_update_smem(a, b, tr); }, 16);
   const int G = (int)((N + TR - 1) / TR);
-  ts_update_kernel<<<G, TS_THREADS, ts_update_smem(a, b, TR), ctx->stream>>>(In, b, A, a, C, ldc, S, Out, N, TR);
-  ctx->launches++;
-  XATU_CK_LAUNCH("ts_update_kernel");
+  XATU_CHAIN(ts_update_kernel, G, TS_THREADS, ts_update_smem(a, b, TR), In, b, A, a, C, ldc, S, Out, N, TR);
   return XATU_OK;
 }
 
@@ -400,14 +406,10 @@ static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int n
     XATU_TRY(ts_update(ctx, t, nsel, V, m, Z, ldZ, nullptr, t, N));
   }
   XATU_TRY(ts_proj(ctx, V, m + nsel, t, nsel, N, Z, ldZ));
-  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(m, nsel), ctx->stream>>>(Z, ldZ, m, nsel, 1e-20, S, dkept);
-  ctx->launches++;
-  XATU_CK_LAUNCH("ts_gram_orth_kernel");
+  XATU_CHAIN(ts_gram_orth_kernel, 1, 32, ts_gram_orth_smem(m, nsel), Z, ldZ, m, nsel, 1e-20, S, dkept);
   XATU_TRY(ts_update(ctx, t, nsel, m > 0 ? V : nullptr, m, Z, ldZ, S, X, N));
   XATU_TRY(ts_proj(ctx, X, nsel, X, nsel, N, Z, ldZ));
-  ts_gram_orth_kernel<<<1, 32, ts_gram_orth_smem(0, nsel), ctx->stream>>>(Z, ldZ, 0, nsel, 1e-24, S, dkept);
-  ctx->launches++;
-  XATU_CK_LAUNCH("ts_gram_orth_kernel");
+  XATU_CHAIN(ts_gram_orth_kernel, 1, 32, ts_gram_orth_smem(0, nsel), Z, ldZ, 0, nsel, 1e-24, S, dkept);
   XATU_TRY(ts_update(ctx, X, nsel, nullptr, 0, nullptr, 0, S, t, N));
   return XATU_OK;
 }
@@ -519,34 +521,23 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_TRY(ts_proj(ctx, V, m, W + (long long)m0 * N, nnew, N, T + (long long)m0 * ldT, ldT));
     {
       const int tot = nnew * m;
-      dav_hermitize_kernel<<<(tot + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, m, m0);
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
-      dav_dead_kernel<<<1, 128, 0, ctx->stream>>>(T, ldT, m, m0, dkept, theta + 769);
-      ctx->launches++;
-      XATU_CK_LAUNCH("dav_dead_kernel");
+      XATU_CHAIN(dav_hermitize_kernel, (tot + 127) / 128, 128, 0, T, ldT, m, m0);
+      XATU_CHAIN(dav_dead_kernel, 1, 128, 0, T, ldT, m, m0, dkept, theta + 769);
     }
     // 3. Rayleigh-Ritz: the lowest nritz eigenpairs of T
     const int nritz = std::min(bsz, m);
-    dav_heev_kernel<<<1, HEEV_THREADS, heev_smem_bytes(m, nritz), ctx->stream>>>(T, ldT, m, nritz, theta, Yr, ldT,
-                                                                                  refl, ctx->d_status.as<int>(), nullptr);
-    ctx->launches++;
-    XATU_CK(cudaGetLastError());
+    XATU_CHAIN(dav_heev_kernel, 1, HEEV_THREADS, heev_smem_bytes(m, nritz), T, ldT, m, nritz, theta, Yr, ldT, refl,
+               ctx->d_status.as<int>(), nullptr);
     // 4. Ritz vectors and residuals
     {
       const int TR = ts_ritz_smem(m, nritz, 64) <= 100 * 1024 ? 64 : 32;
       const int G = (int)((N + TR - 1) / TR);
       XATU_TRY(ts_part_ensure(ctx, (size_t)G * nritz * sizeof(cd)));
-      ts_ritz_kernel<<<G, TS_THREADS, ts_ritz_smem(m, nritz, TR), ctx->stream>>>(
-          V, W, m, Yr, ldT, nritz, theta, diagH, N, TR, U, WU, P, ctx->dv_part.as<cd>());
-      ctx->launches++;
-      XATU_CK_LAUNCH("ts_ritz_kernel");
+      XATU_CHAIN(ts_ritz_kernel, G, TS_THREADS, ts_ritz_smem(m, nritz, TR), V, W, m, Yr, ldT, nritz, theta, diagH, N,
+                 TR, U, WU, P, ctx->dv_part.as<cd>());
       // squared residual norms as complex pairs at [256, 256 + 2 nritz), the status word at 768
-      ts_sum_kernel<<<(nritz + 31) / 32, TS_SUM_THREADS, 0, ctx->stream>>>(ctx->dv_part.as<cd>(), G, nritz, nritz,
-                                                                         reinterpret_cast<cd*>(norms), 1,
-                                                                         ctx->d_status.as<int>(), theta + 768);
-      ctx->launches++;
-      XATU_CK_LAUNCH("ts_sum_kernel");
+      XATU_CHAIN(ts_sum_kernel, (nritz + 31) / 32, TS_SUM_THREADS, 0, ctx->dv_part.as<cd>(), G, nritz, nritz,
+                 reinterpret_cast<cd*>(norms), 1, ctx->d_status.as<int>(), theta + 768);
     }
     // one read-back: theta [0, 256), residual norms [256, 512), status word at 768, kept columns of the
     // newest block at 769
@@ -588,9 +579,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     if (m + nsel > mmax) {
       XATU_CK(cudaMemcpyAsync(V, U, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
       XATU_CK(cudaMemcpyAsync(W, WU, sizeof(cd) * (size_t)N * nritz, cudaMemcpyDeviceToDevice, ctx->stream));
-      dav_set_diag_kernel<<<(nritz * nritz + 127) / 128, 128, 0, ctx->stream>>>(T, ldT, nritz, theta);
-      ctx->launches++;
-      XATU_CK(cudaGetLastError());
+      XATU_CHAIN(dav_set_diag_kernel, (nritz * nritz + 127) / 128, 128, 0, T, ldT, nritz, theta);
       m = nritz;
       dead = 0;
       if (m + nsel > mmax) nsel = mmax - m;
@@ -599,10 +588,8 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(cudaMemcpyAsync(sel_dev, sel.data(), nsel * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     {
       const long long tot = N * nsel;
-      ts_gather_kernel<<<(int)((tot + threads - 1) / threads), threads, 0, ctx->stream>>>(P, sel_dev, nsel, N,
-                                                                                          V + (long long)m * N);
-      ctx->launches++;
-      XATU_CK_LAUNCH("ts_gather_kernel");
+      XATU_CHAIN(ts_gather_kernel, (int)((tot + threads - 1) / threads), threads, 0, P, sel_dev, nsel, N,
+                 V + (long long)m * N);
     }
     XATU_TRY(orthonormalize_block(ctx, N, m, nsel));
     m0 = m;

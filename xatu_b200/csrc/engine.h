@@ -184,6 +184,25 @@ xatu_status xatu_apply_h(xatu_ctx* ctx, long long N, int col0, int nv);
 void xatu_hx_collect(xatu_ctx* ctx);
 
 // After a kernel launch: the launch's own error, labelled with the kernel.
+// Launch of a kernel that begins with xatu_grid_chain(): programmatic stream serialisation, so that the
+// kernel is scheduled while its predecessor on the stream finishes (the launch latency of the short
+// Davidson kernels overlaps the tail of the previous one).
+template <typename... KArgs, typename... Args>
+inline cudaError_t xatu_launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 #define XATU_CK_LAUNCH(name)                                                       \
   do {                                                                             \
     cudaError_t e__ = cudaGetLastError();                                          \

@@ -446,6 +446,7 @@ hx_herm_tcgen05_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_
 __global__ void hx_operand_kernel(const cd* __restrict__ X, long long ldx, long long N, int b, int bp, long long ldb,
                                   long long ldu, __nv_bfloat16* __restrict__ Bhi, __nv_bfloat16* __restrict__ Blo,
                                   __nv_bfloat16* __restrict__ Uhi, __nv_bfloat16* __restrict__ Ulo) {
+  xatu_grid_chain();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= N * bp) return;
   const int s = (int)(t / N);
@@ -478,10 +479,9 @@ cudaError_t xatu_launch_hx_operands(const cd* X, long long ldx, long long N, int
                                     long long ldb, void* Uhi, void* Ulo, long long ldu, cudaStream_t s) {
   if (b > bp || ldb < 2 * N || ldu < N) return cudaErrorInvalidValue;
   const long long tot = N * bp;
-  hx_operand_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
-      X, ldx, N, b, bp, ldb, ldu, static_cast<__nv_bfloat16*>(Bhi), static_cast<__nv_bfloat16*>(Blo),
-      static_cast<__nv_bfloat16*>(Uhi), static_cast<__nv_bfloat16*>(Ulo));
-  return cudaGetLastError();
+  return xatu_launch_chained(hx_operand_kernel, dim3((unsigned)((tot + 255) / 256)), dim3(256), 0, s, X, ldx, N, b, bp,
+                             ldb, ldu, static_cast<__nv_bfloat16*>(Bhi), static_cast<__nv_bfloat16*>(Blo),
+                             static_cast<__nv_bfloat16*>(Uhi), static_cast<__nv_bfloat16*>(Ulo));
 }
 
 // ------------------------------------------------------------------ host side
