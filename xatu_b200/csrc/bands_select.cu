@@ -8,9 +8,11 @@
 // ExcitonTB.cpp:673-683).
 //
 // One warp per k point: the H(R) blocks are staged once per CTA (cp.async,
-// double-buffered) and accumulated by every warp with its own Bloch phases;
-// then Householder reduction to real tridiagonal form in the warp (one row of
-// the lower triangle per lane), Sturm-sequence multisection for the wanted
+// double-buffered) and accumulated by every warp with its own Bloch phases
+// into the packed lower triangle of H(k) (row r at r(r+1)/2; 4 KB per warp at
+// 22 orbitals, so that up to 25 warps fit one SM and a mesh of 3600 k points
+// runs in one wave); then Householder reduction to real tridiagonal form in
+// the warp (one row of the lower triangle per lane), Sturm-sequence multisection for the wanted
 // ranks (a group of lanes per eigenvalue), inverse iteration with cluster
 // orthonormalisation for the eigenvectors (one lane per eigenvector), and the
 // back-transformation by the stored reflectors.  The algorithms are those of
@@ -19,68 +21,90 @@
 #include "bands.cuh"
 #include "eigh_small.cuh"
 
-#define BS_MAXW 8
+// Largest warps per CTA of each instantiation: 25 for the 4-band window (72 registers; 3600 k points fill
+// 148 SMs in one wave), 8 for the wider windows (128 and 255 registers).
+template <int NBS>
+struct BsMaxW {
+  static constexpr int value = NBS == 4 ? 25 : 8;
+};
+
+// Packed lower triangle: element (r, c), c <= r.
+__device__ __forceinline__ int bs_tri(int r, int c) { return ((r * (r + 1)) >> 1) + c; }
 
 __device__ __forceinline__ void ts_cp16_bs(cd* dst, const cd* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
 
+// Per-warp shared memory.  Arrays live in phases and share space where their phases do not overlap:
+// the Bloch phases (H(k) sum) with the inverse-iteration factors, the reflector v and p (reduction) with
+// the tridiagonal eigenvectors Z, e^2 (multisection) with the cluster Gram matrix (inverse iteration).
 struct BsLayout {
   size_t stage;      // two staged H(R) blocks
   size_t per_warp;
-  int lda;
+  size_t oR1, oU2, oTau, oD, oE, oU3, oLam, oPM, oInt;   // offsets from the warp's base; A at 0
 };
+
+__host__ __device__ inline size_t bs_max(size_t a, size_t b) { return a > b ? a : b; }
 
 __host__ __device__ inline BsLayout bs_layout(int n, int nR, int nbs) {
   BsLayout L;
-  L.lda = band_lda(n);
   L.stage = (size_t)2 * n * n * sizeof(cd);
-  size_t w = (size_t)n * L.lda * sizeof(cd);      // A
-  w += (size_t)nR * sizeof(cd);                    // phases
-  w += (size_t)3 * n * sizeof(cd);                 // v, p, tau
-  w += (size_t)3 * n * sizeof(double);             // d, e, e^2
-  w += (size_t)nbs * sizeof(double);               // lam
-  w += (size_t)n * nbs * sizeof(double);           // Z
-  w += (size_t)4 * n * nbs * sizeof(double);       // LU factors
-  w += (size_t)nbs * nbs * sizeof(double);         // Gram
-  w += (size_t)n * sizeof(unsigned);               // row-swap masks
-  w += (size_t)3 * nbs * sizeof(int) + 16;         // order, clusters, flags
+  size_t w = (size_t)n * (n + 1) / 2 * sizeof(cd);                                    // A, packed lower triangle
+  L.oR1 = w;
+  w += bs_max((size_t)nR * sizeof(cd), (size_t)4 * n * nbs * sizeof(double));         // phases | LU factors
+  L.oU2 = w;
+  w += bs_max((size_t)2 * n * sizeof(cd), (size_t)n * nbs * sizeof(double));         // v, p | Z
+  L.oTau = w;
+  w += (size_t)n * sizeof(cd);                                                        // tau
+  L.oD = w;
+  w += (size_t)n * sizeof(double);                                                    // d
+  L.oE = w;
+  w += (size_t)n * sizeof(double);                                                    // e
+  L.oU3 = w;
+  w += bs_max((size_t)n * sizeof(double), (size_t)nbs * nbs * sizeof(double));        // e^2 | Gram
+  L.oLam = w;
+  w += (size_t)nbs * sizeof(double);                                                  // lam
+  L.oPM = w;
+  w += (size_t)n * sizeof(unsigned);                                                  // row-swap masks
+  w = (w + 15) / 16 * 16;
+  L.oInt = w;
+  w += (size_t)3 * nbs * sizeof(int) + 16;                                            // order, clusters, flags
   L.per_warp = (w + 15) / 16 * 16;
   return L;
 }
 
 template <int NBS>
-__global__ void __launch_bounds__(BS_MAXW * 32)
+__global__ void __launch_bounds__(BsMaxW<NBS>::value * 32)
 band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const double* __restrict__ cellsR,
                    const cd* __restrict__ HR, double* __restrict__ eigval, cd* __restrict__ eigvec,
                    int* __restrict__ status, int wpc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = bp.norb, nR = bp.nR, nb = bp.nb, nn = n * n;
   const BsLayout Ly = bs_layout(n, nR, NBS);
-  const int lda = Ly.lda;
+  const int np = n * (n + 1) / 2;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k = blockIdx.x * wpc + warp;
   const bool kval = k < bp.nk;
   cd* HRs = reinterpret_cast<cd*>(smem_raw);   // [2][n * n]
   unsigned char* wb = smem_raw + Ly.stage + (size_t)warp * Ly.per_warp;
-  cd* A = reinterpret_cast<cd*>(wb);
-  cd* ph = A + n * lda;
-  cd* sv = ph + nR;
-  cd* sp = sv + n;
-  cd* stau = sp + n;
-  double* sd = reinterpret_cast<double*>(stau + n);
-  double* se = sd + n;
-  double* se2 = se + n;
-  double* lam = se2 + n;
-  double* Z = lam + NBS;                     // n x NBS
-  double* RI = Z + n * NBS;                  // [n][NBS]
+  cd* A = reinterpret_cast<cd*>(wb);                           // packed lower triangle (bs_tri)
+  cd* ph = reinterpret_cast<cd*>(wb + Ly.oR1);                 // Bloch phases (H(k) sum only)
+  double* RI = reinterpret_cast<double*>(wb + Ly.oR1);         // [n][NBS] LU factors (inverse iteration only)
   double* DU = RI + n * NBS;
   double* DU2 = DU + n * NBS;
   double* FM = DU2 + n * NBS;
-  double* G = FM + n * NBS;                  // NBS x NBS
-  unsigned* PM = reinterpret_cast<unsigned*>(G + NBS * NBS);
-  int* ord = reinterpret_cast<int*>(PM + n);   // slots in ascending rank
+  cd* sv = reinterpret_cast<cd*>(wb + Ly.oU2);                 // reflector v, p (reduction only)
+  cd* sp = sv + n;
+  double* Z = reinterpret_cast<double*>(wb + Ly.oU2);          // n x NBS (after the multisection)
+  cd* stau = reinterpret_cast<cd*>(wb + Ly.oTau);
+  double* sd = reinterpret_cast<double*>(wb + Ly.oD);
+  double* se = reinterpret_cast<double*>(wb + Ly.oE);
+  double* se2 = reinterpret_cast<double*>(wb + Ly.oU3);        // multisection only
+  double* G = reinterpret_cast<double*>(wb + Ly.oU3);          // NBS x NBS (inverse iteration only)
+  double* lam = reinterpret_cast<double*>(wb + Ly.oLam);
+  unsigned* PM = reinterpret_cast<unsigned*>(wb + Ly.oPM);
+  int* ord = reinterpret_cast<int*>(wb + Ly.oInt);   // slots in ascending rank
   int* cl = ord + NBS;
   int* flg = cl + NBS;
   const double eps = 2.220446049250313e-16;
@@ -94,7 +118,13 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
     sincos(kx * cellsR[3 * r] + ky * cellsR[3 * r + 1] + kz * cellsR[3 * r + 2], &sn, &cs);
     ph[r] = mk(cs, sn);
   }
-  for (int t = lane; t < nn; t += 32) A[(t / n) * lda + (t % n)] = mk(0, 0);
+  for (int t = lane; t < np; t += 32) A[t] = mk(0, 0);
+  // (row, column) of this lane's first packed entry; the lane then steps 32 entries at a time
+  int r0 = (int)((sqrt(8.0 * lane + 1.0) - 1.0) * 0.5);
+  while ((r0 + 1) * (r0 + 2) / 2 <= lane) r0++;
+  while (r0 * (r0 + 1) / 2 > lane) r0--;
+  const int c0 = lane - r0 * (r0 + 1) / 2;
+  const bool tri = bp.triangular;
   for (int t = threadIdx.x; t < nn; t += blockDim.x) ts_cp16_bs(HRs + t, HR + t);
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   for (int r = 0; r < nR; r++) {
@@ -106,40 +136,33 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 1;\n" ::: "memory");
     __syncthreads();
     const cd f = ph[r];
-    for (int t = lane; t < nn; t += 32) {
-      cd& a = A[(t / n) * lda + (t % n)];
-      a = a + cur[t] * f;
+    // lower triangle of H(k); in triangular storage H(k) = h + h^H (h the lower-triangular sum with half its
+    // diagonal): entry (i, j) takes h_ij + conj(h_ji), the diagonal the real part of h_ii
+    int i = r0, j = c0;
+    for (int t = lane; t < np; t += 32) {
+      const cd a = cur[i * n + j] * f;
+      cd add;
+      if (!tri) add = a;
+      else if (i == j) add = mk(a.x, 0.0);
+      else add = a + conj(cur[j * n + i] * f);
+      A[t] = A[t] + add;
+      j += 32;
+      while (j > i) {
+        j -= i + 1;
+        i++;
+      }
     }
     __syncthreads();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   if (!kval) return;   // no CTA-wide barrier below this point
   __syncwarp();
-  if (bp.triangular) {
-    // h.diag() -= h.diag()/2; h += h^dagger (lower triangle kept)
-    for (int t = lane; t < nn; t += 32) {
-      const int i = t / n, j = t % n;
-      if (j > i) continue;
-      const cd a = A[i * lda + j], b = A[j * lda + i];
-      cd v;
-      if (i == j) {
-        const cd dh = mk(a.x - a.x / 2, a.y - a.y / 2);
-        v = dh + conj(dh);
-      } else {
-        v = a + conj(b);
-      }
-      A[i * lda + j] = v;
-    }
-  } else {
-    for (int i = lane; i < n; i += 32) A[i * lda + i].y = 0.0;
-  }
+  if (!tri)
+    for (int i = lane; i < n; i += 32) A[bs_tri(i, i)].y = 0.0;
   __syncwarp();
   {
     bool fin = true;
-    for (int t = lane; t < nn; t += 32) {
-      const int i = t / n, j = t % n;
-      if (j <= i) fin = fin && isfinite(A[i * lda + j].x) && isfinite(A[i * lda + j].y);
-    }
+    for (int t = lane; t < np; t += 32) fin = fin && isfinite(A[t].x) && isfinite(A[t].y);
     if (!__all_sync(0xffffffffu, fin)) {
       if (lane == 0) atomicOr(status, XATU_DEVERR_NAN);
       return;
@@ -150,9 +173,9 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
   for (int j = 0; j < n - 1; j++) {
     const int L = n - j - 1;
     double s = 0.0;
-    for (int i = 1 + lane; i < L; i += 32) s += nrm2(A[(j + 1 + i) * lda + j]);
+    for (int i = 1 + lane; i < L; i += 32) s += nrm2(A[bs_tri(j + 1 + i, j)]);
     s = heev_wsum(s);
-    const cd al = A[(j + 1) * lda + j];
+    const cd al = A[bs_tri(j + 1, j)];
     cd tau = mk(0, 0), scal = mk(0, 0);
     double beta = al.x;
     const bool on = (s > 0.0 || al.y != 0.0);
@@ -165,14 +188,14 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
       scal = mk(den.x * rdn, -den.y * rdn);
     }
     for (int i = lane; i < L; i += 32) {
-      cd vi = (i == 0) ? mk(1.0, 0.0) : (on ? A[(j + 1 + i) * lda + j] * scal : mk(0, 0));
+      cd vi = (i == 0) ? mk(1.0, 0.0) : (on ? A[bs_tri(j + 1 + i, j)] * scal : mk(0, 0));
       sv[i] = vi;
-      if (i >= 1) A[(j + 1 + i) * lda + j] = vi;
+      if (i >= 1) A[bs_tri(j + 1 + i, j)] = vi;
     }
     if (lane == 0) {
       stau[j] = tau;
       se[j] = beta;
-      sd[j] = A[j * lda + j].x;
+      sd[j] = A[bs_tri(j, j)].x;
     }
     __syncwarp();
     if (!on) continue;
@@ -182,16 +205,16 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
       int l = 0;
       for (; l + 1 < L; l += 2) {
         const int g0 = j + 1 + l, g1 = g0 + 1;
-        cd a0 = A[l <= i ? gr * lda + g0 : g0 * lda + gr];
+        cd a0 = A[l <= i ? bs_tri(gr, g0) : bs_tri(g0, gr)];
         if (l > i) a0.y = -a0.y;
-        cd a1 = A[l + 1 <= i ? gr * lda + g1 : g1 * lda + gr];
+        cd a1 = A[l + 1 <= i ? bs_tri(gr, g1) : bs_tri(g1, gr)];
         if (l + 1 > i) a1.y = -a1.y;
         acc0 = acc0 + a0 * sv[l];
         acc1 = acc1 + a1 * sv[l + 1];
       }
       if (l < L) {
         const int g0 = j + 1 + l;
-        cd a0 = A[l <= i ? gr * lda + g0 : g0 * lda + gr];
+        cd a0 = A[l <= i ? bs_tri(gr, g0) : bs_tri(g0, gr)];
         if (l > i) a0.y = -a0.y;
         acc0 = acc0 + a0 * sv[l];
       }
@@ -209,7 +232,7 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
     const double K = 0.5 * (tau.x * sx + tau.y * sy);
     for (int i = lane; i < L; i += 32) {
       const cd vi = sv[i], wi = sp[i] - K * vi;
-      cd* Ar = A + (j + 1 + i) * lda + (j + 1);
+      cd* Ar = A + bs_tri(j + 1 + i, j + 1);
       for (int l = 0; l <= i; l++) {
         const cd vl = sv[l], wl = sp[l] - K * vl;
         Ar[l] = Ar[l] - (vi * conj(wl) + wi * conj(vl));
@@ -218,7 +241,7 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
     __syncwarp();
   }
   if (lane == 0) {
-    sd[n - 1] = A[(n - 1) * lda + (n - 1)].x;
+    sd[n - 1] = A[bs_tri(n - 1, n - 1)].x;
     se[n - 1] = 0.0;
   }
   __syncwarp();
@@ -441,7 +464,7 @@ band_select_kernel(BandParams bp, const double* __restrict__ kpoints, const doub
 #pragma unroll
     for (int pq = 0; pq < PER; pq++) {
       const int row = lane + 32 * pq;
-      vr[pq] = (row < n && row > r) ? (row == r + 1 ? mk(1.0, 0.0) : A[row * lda + r]) : mk(0, 0);
+      vr[pq] = (row < n && row > r) ? (row == r + 1 ? mk(1.0, 0.0) : A[bs_tri(row, r)]) : mk(0, 0);
     }
     double sx[NBS], sy[NBS];
 #pragma unroll
@@ -513,7 +536,8 @@ extern "C" cudaError_t xatu_launch_band_select(const BandParams& bp, const doubl
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int wmax = 1;
-  while (wmax < BS_MAXW && Ly.stage + (size_t)(wmax + 1) * Ly.per_warp <= max_smem) wmax++;
+  const int maxw = nbs == 4 ? BsMaxW<4>::value : (nbs == 8 ? BsMaxW<8>::value : BsMaxW<16>::value);
+  while (wmax < maxw && Ly.stage + (size_t)(wmax + 1) * Ly.per_warp <= max_smem) wmax++;
   cudaError_t e = xatu_raise_smem_limit(fn, Ly.stage + (size_t)wmax * Ly.per_warp);
   if (e != cudaSuccess) return e;
   int wpc = 1;
