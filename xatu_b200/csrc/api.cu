@@ -108,7 +108,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->d_adjdtable, &ctx->d_adjdVX, &ctx->d_adjAlpha, &ctx->d_adjExUW, &ctx->d_adjCbar,
                   &ctx->d_adjEbar, &ctx->d_adjEpart, &ctx->d_adjGk, &ctx->d_adjG, &ctx->d_oscG,
                   &ctx->dv_part, &ctx->d_pp_X, &ctx->d_pp_A, &ctx->d_pp_B, &ctx->d_pp_C, &ctx->d_pp_D,
-                  &ctx->d_pp_P, &ctx->d_pp_E};
+                  &ctx->d_pp_P, &ctx->d_pp_E, &ctx->d_mesh_int, &ctx->d_cells_int};
   for (DBuf* b : bufs) b->release();
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
   if (ctx->blas) cublasDestroy(ctx->blas);
@@ -321,9 +321,48 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
   if (ctx->mode == XATU_MODE_RECIPROCAL && !ctx->kgrid_ok)
     return xatu_fail(ctx, XATU_ERR_UNSUPPORTED,
                      "reciprocal-space mode needs k points on a regular grid of the (ncell*factor) mesh");
+  // integer coordinates of the BZ mesh (q = sum_d m_d / n_eff b_d) and of the cells (R = sum_d n_d a_d,
+  // n_d = b_d.R / 2 pi), for the root-of-unity phases of the motif FT
+  ctx->ft_roots = ctx->mode == XATU_MODE_REALSPACE && n_eff <= XATU_FT_MAXDEN;
+  if (ctx->ft_roots) {
+    const int nd = ctx->ndim;
+    ctx->mesh_int.assign(3 * (size_t)nmesh, 0);
+    for (long long i = 0; i < nmesh && ctx->ft_roots; i++) {
+      const double* q = ctx->mesh.data() + 3 * i;
+      double ind[3] = {0, 0, 0};
+      for (int a = 0; a < nd; a++)
+        ind[a] = ctx->recip[3 * a] * q[0] + ctx->recip[3 * a + 1] * q[1] + ctx->recip[3 * a + 2] * q[2];
+      for (int a = 0; a < nd; a++) {
+        double red = 0.0;
+        for (int b = 0; b < nd; b++) red += ctx->inv_gram[a * nd + b] * ind[b];
+        red *= n_eff;
+        const double u = std::round(red);
+        if (std::fabs(red - u) > 1e-6) ctx->ft_roots = false;
+        ctx->mesh_int[3 * i + a] = (int)u;
+      }
+    }
+    const size_t ncl = ctx->cells.size() / 3;
+    ctx->cells_int.assign(3 * ncl, 0);
+    for (size_t i = 0; i < ncl && ctx->ft_roots; i++) {
+      const double* R = ctx->cells.data() + 3 * i;
+      for (int a = 0; a < nd; a++) {
+        const double f = (ctx->recip[3 * a] * R[0] + ctx->recip[3 * a + 1] * R[1] + ctx->recip[3 * a + 2] * R[2]) /
+                         (2.0 * XATU_PI);
+        const double u = std::round(f);
+        if (std::fabs(f - u) > 1e-6) ctx->ft_roots = false;
+        long long v = (long long)u % n_eff;
+        if (v < 0) v += n_eff;
+        ctx->cells_int[3 * i + a] = (int)v;
+      }
+    }
+  }
   XATU_CK(upload(ctx->d_kpoints, ctx->kpoints.data(), ctx->kpoints.size(), ctx->stream));
   XATU_CK(upload(ctx->d_mesh, ctx->mesh.data(), ctx->mesh.size(), ctx->stream));
   XATU_CK(upload(ctx->d_cells, ctx->cells.data(), ctx->cells.size(), ctx->stream));
+  if (ctx->ft_roots) {
+    XATU_CK(upload(ctx->d_mesh_int, ctx->mesh_int.data(), ctx->mesh_int.size(), ctx->stream));
+    XATU_CK(upload(ctx->d_cells_int, ctx->cells_int.data(), ctx->cells_int.size(), ctx->stream));
+  }
   XATU_CK(upload(ctx->d_G, ctx->G.data(), ctx->G.size(), ctx->stream));
   XATU_CK(upload(ctx->d_kgrid, ctx->kgrid.data(), ctx->kgrid.size(), ctx->stream));
   {
@@ -515,12 +554,20 @@ xatu_status xatu_tables_enqueue(xatu_ctx* ctx) {
     ctx->launches++;
     XATU_CK_LAUNCH("pair_potential_kernel");
     dim3 g2(ctx->nmesh, (npairs + 7) / 8);
-    motif_ft_kernel<<<g2, 256, 0, ctx->stream>>>(ctx->nmesh, ctx->d_mesh.as<double>(), ncells,
-                                                 ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
-                                                 ctx->d_vtab.as<double>(), 1.0 / ctx->total_cells, na,
-                                                 ctx->d_table.as<cd>());
-    ctx->launches++;
-    XATU_CK_LAUNCH("motif_ft_kernel");
+    if (ctx->ft_roots) {
+      motif_ft_roots_kernel<<<g2, 256, (size_t)ctx->n_eff * sizeof(double2), ctx->stream>>>(
+          ctx->nmesh, ctx->d_mesh_int.as<int>(), ctx->n_eff, ncells, ctx->d_cells_int.as<int>(), npairs,
+          ctx->d_pairs.as<int2>(), ctx->d_vtab.as<double>(), 1.0 / ctx->total_cells, na, ctx->d_table.as<cd>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("motif_ft_roots_kernel");
+    } else {
+      motif_ft_kernel<<<g2, 256, 0, ctx->stream>>>(ctx->nmesh, ctx->d_mesh.as<double>(), ncells,
+                                                   ctx->d_cells.as<double>(), npairs, ctx->d_pairs.as<int2>(),
+                                                   ctx->d_vtab.as<double>(), 1.0 / ctx->total_cells, na,
+                                                   ctx->d_table.as<cd>());
+      ctx->launches++;
+      XATU_CK_LAUNCH("motif_ft_kernel");
+    }
     if (ctx->exchange) {
       const double* vt = ctx->d_vtab.as<double>();
       if (ctx->exchange_potential != ctx->potential) {

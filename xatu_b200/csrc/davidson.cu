@@ -74,12 +74,15 @@ __device__ __forceinline__ double dav_noise(unsigned long long i, unsigned long 
 __device__ __forceinline__ bool dav_sel_less(double a, long long ia, double b, long long ib) {
   return a < b || (a == b && ia < ib);
 }
+#define DAV_SEL_SMEM_ROWS 24576   // diagonals up to this length are worked on in shared memory (192 KB)
 __global__ void __launch_bounds__(DAV_SEL_THREADS)
-dav_select_lowest_kernel(const double* __restrict__ d, long long N, int nsel, double* __restrict__ w,
+dav_select_lowest_kernel(const double* __restrict__ d, long long N, int nsel, double* __restrict__ wg,
                          int* __restrict__ idx, int* __restrict__ kept) {
+  extern __shared__ double ws[];
   __shared__ double sv[DAV_SEL_THREADS / 32];
   __shared__ long long si[DAV_SEL_THREADS / 32];
   __shared__ long long win;
+  double* w = N <= DAV_SEL_SMEM_ROWS ? ws : wg;   // working copy of the diagonal (winners set to +inf)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   double best = INFINITY;
   long long bi = N;
@@ -472,9 +475,12 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     XATU_CK(cudaGetLastError());
   }
   // start columns: the bsz lowest diagonal entries, chosen on the device (no host round trip)
-  dav_select_lowest_kernel<<<1, DAV_SEL_THREADS, 0, ctx->stream>>>(diagH, N, bsz,
-                                                                   reinterpret_cast<double*>(ctx->dv_tmp.p), sel_dev,
-                                                                   dkept);
+  {
+    const size_t sel_smem = N <= DAV_SEL_SMEM_ROWS ? (size_t)N * sizeof(double) : 0;
+    XATU_CK(xatu_raise_smem_limit((const void*)dav_select_lowest_kernel, DAV_SEL_SMEM_ROWS * sizeof(double)));
+    dav_select_lowest_kernel<<<1, DAV_SEL_THREADS, sel_smem, ctx->stream>>>(
+        diagH, N, bsz, reinterpret_cast<double*>(ctx->dv_tmp.p), sel_dev, dkept);
+  }
   ctx->launches++;
   XATU_CK(cudaGetLastError());
   {

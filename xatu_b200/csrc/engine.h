@@ -69,6 +69,11 @@ struct xatu_ctx {
   std::vector<double> kpoints, mesh, cells, G;
   std::vector<int> kgrid;
   bool kgrid_ok = false;
+  // integer coordinates of the mesh (units b_d / n_eff) and of the cells (units a_d, reduced mod n_eff) when
+  // both are commensurate; the motif FT then takes its phases from a table of roots of unity
+  std::vector<int> mesh_int, cells_int;
+  bool ft_roots = false;
+  DBuf d_mesh_int, d_cells_int;
   int rt_len[3] = {1, 1, 1}, rt_span[3] = {0, 0, 0};
   long long rt_entries = 1;
   DBuf d_kpoints, d_mesh, d_cells, d_G, d_kgrid, d_basis, d_Q;

@@ -7,6 +7,10 @@ extern "C" __global__ void pair_potential_kernel(PotParams p, int kind, int deri
                                                  double* vtab);
 extern "C" __global__ void motif_ft_kernel(int nq, const double* q, int ncells, const double* cells, int npairs,
                                            const int2* pairs, const double* vtab, double inv_total, int na, cd* out);
+extern "C" __global__ void motif_ft_roots_kernel(int nq, const int* mi, int den, int ncells, const int* ni,
+                                                 int npairs, const int2* pairs, const double* vtab, double inv_total,
+                                                 int na, cd* out);
+#define XATU_FT_MAXDEN 3072   // largest mesh denominator of the root-of-unity table (48 KB of shared memory)
 extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int deriv, int nentries, const double* G,
                                               int na, const double* motif, cd* W);
 extern "C" __global__ void exchange_vectors_kernel(int N, int nv, int nc, int nb, int norb, int na, const int* orb_off,

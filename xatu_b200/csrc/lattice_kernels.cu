@@ -10,6 +10,9 @@
 //                            One CTA per (q, chunk of pairs); the phase e^{iq.R}
 //                            is computed once per cell and reused by every pair;
 //                            warp-shuffle + shared-memory reduction.
+//                            motif_ft_roots_kernel: the same sum when the mesh
+//                            and the cells are commensurate (a Monkhorst-Pack
+//                            mesh and lattice cells), the phase a table lookup.
 //  * recip_table_kernel      W_ab(q) = sum_G Vt(q + G) e^{i (q+G).(tau_a - tau_b)}
 //                            over the table of k - k' differences of a grid of k
 //                            points.  It carries the reciprocal-space interaction
@@ -77,6 +80,66 @@ motif_ft_kernel(int nq, const double* __restrict__ q, int ncells, const double* 
         const double v = vtab[(int64_t)(p0 + j) * ncells + n];
         accr[j] = fma(v, c, accr[j]);
         acci[j] = fma(v, s, acci[j]);
+      }
+    }
+  }
+  __shared__ double red[2][MOTIF_PAIR_CHUNK][MOTIF_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
+    const double r = warp_sum(accr[j]);
+    const double i = warp_sum(acci[j]);
+    if (lane == 0) { red[0][j][warp] = r; red[1][j][warp] = i; }
+  }
+  __syncthreads();
+  if (threadIdx.x < np) {
+    const int j = threadIdx.x;
+    double r = 0.0, i = 0.0;
+    for (int w = 0; w < MOTIF_THREADS / 32; w++) { r += red[0][j][w]; i += red[1][j][w]; }
+    r *= inv_total;
+    i *= inv_total;
+    const int2 ab = pairs[p0 + j];
+    cd* o = out + (int64_t)iq * na * na;
+    o[ab.x * na + ab.y] = mk(r, i);
+    o[ab.y * na + ab.x] = mk(r, -i);
+  }
+}
+
+// motif_ft_kernel for a mesh and cells that are commensurate: q = sum_d (m_d / den) b_d and R = sum_d n_d a_d
+// with integers m, n, so that e^{i q.R} = e^{2 pi i (m.n mod den) / den} comes from a table of the den roots of
+// unity (sincospi of exact fractions) instead of one sincos per (q, cell).  mi: nq x 3, ni: ncells x 3,
+// every n_d reduced to [0, den).  Dynamic shared memory: den x 16 bytes.
+extern "C" __global__ void __launch_bounds__(MOTIF_THREADS)
+motif_ft_roots_kernel(int nq, const int* __restrict__ mi, int den, int ncells, const int* __restrict__ ni, int npairs,
+                      const int2* __restrict__ pairs, const double* __restrict__ vtab, double inv_total, int na,
+                      cd* __restrict__ out) {
+  extern __shared__ double2 roots[];
+  const int iq = blockIdx.x;
+  const int p0 = blockIdx.y * MOTIF_PAIR_CHUNK;
+  const int np = min(MOTIF_PAIR_CHUNK, npairs - p0);
+  for (int t = threadIdx.x; t < den; t += blockDim.x) {
+    double s, c;
+    sincospi(2.0 * (double)t / (double)den, &s, &c);
+    roots[t] = make_double2(c, s);
+  }
+  // m_d mod den in [0, den)
+  int m0 = mi[3 * iq] % den, m1 = mi[3 * iq + 1] % den, m2 = mi[3 * iq + 2] % den;
+  m0 += m0 < 0 ? den : 0;
+  m1 += m1 < 0 ? den : 0;
+  m2 += m2 < 0 ? den : 0;
+  __syncthreads();
+  double accr[MOTIF_PAIR_CHUNK], acci[MOTIF_PAIR_CHUNK];
+#pragma unroll
+  for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) { accr[j] = 0.0; acci[j] = 0.0; }
+  for (int n = threadIdx.x; n < ncells; n += blockDim.x) {
+    const int e = (m0 * ni[3 * n] + m1 * ni[3 * n + 1] + m2 * ni[3 * n + 2]) % den;
+    const double2 ph = roots[e];
+#pragma unroll
+    for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
+      if (j < np) {
+        const double v = vtab[(int64_t)(p0 + j) * ncells + n];
+        accr[j] = fma(v, ph.x, accr[j]);
+        acci[j] = fma(v, ph.y, acci[j]);
       }
     }
   }
