@@ -555,7 +555,8 @@ xatu_status xatu_tables_enqueue(xatu_ctx* ctx) {
     XATU_CK_LAUNCH("pair_potential_kernel");
     dim3 g2(ctx->nmesh, (npairs + 7) / 8);
     if (ctx->ft_roots) {
-      motif_ft_roots_kernel<<<g2, 256, (size_t)ctx->n_eff * sizeof(double2), ctx->stream>>>(
+      const dim3 gr((ctx->nmesh + XATU_MOTIF_QB - 1) / XATU_MOTIF_QB, (npairs + 7) / 8);
+      motif_ft_roots_kernel<<<gr, 256, motif_roots_smem(ctx->n_eff), ctx->stream>>>(
           ctx->nmesh, ctx->d_mesh_int.as<int>(), ctx->n_eff, ncells, ctx->d_cells_int.as<int>(), npairs,
           ctx->d_pairs.as<int2>(), ctx->d_vtab.as<double>(), 1.0 / ctx->total_cells, na, ctx->d_table.as<cd>());
       ctx->launches++;

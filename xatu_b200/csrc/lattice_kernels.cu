@@ -23,7 +23,7 @@
 //                            so that the exchange term is X_ij = sum_a L_a(i) R_a(j)
 //                            (realSpaceInteractionTerm with (c_k, v'_k', v_k, c'_k'),
 //                            ExcitonTB.cpp:897, and its reciprocal form :905).
-#include "params.h"
+#include "kernels.h"
 
 #define MOTIF_PAIR_CHUNK 8
 #define MOTIF_THREADS 256
@@ -107,14 +107,22 @@ motif_ft_kernel(int nq, const double* __restrict__ q, int ncells, const double* 
 
 // motif_ft_kernel for a mesh and cells that are commensurate: q = sum_d (m_d / den) b_d and R = sum_d n_d a_d
 // with integers m, n, so that e^{i q.R} = e^{2 pi i (m.n mod den) / den} comes from a table of the den roots of
-// unity (sincospi of exact fractions) instead of one sincos per (q, cell).  mi: nq x 3, ni: ncells x 3,
-// every n_d reduced to [0, den).  Dynamic shared memory: den x 16 bytes.
+// unity (sincospi of exact fractions) instead of one sincos per (q, cell).  One CTA per MOTIF_QB mesh points
+// (16 threads each) and chunk of pairs: the potentials of a chunk of cells are staged in shared memory once and
+// used by all of the CTA's points.  mi: nq x 3, ni: ncells x 3, every n_d reduced to [0, den).
+// Dynamic shared memory: motif_roots_smem(den).
+#define MOTIF_QB XATU_MOTIF_QB
 extern "C" __global__ void __launch_bounds__(MOTIF_THREADS)
 motif_ft_roots_kernel(int nq, const int* __restrict__ mi, int den, int ncells, const int* __restrict__ ni, int npairs,
                       const int2* __restrict__ pairs, const double* __restrict__ vtab, double inv_total, int na,
                       cd* __restrict__ out) {
-  extern __shared__ double2 roots[];
-  const int iq = blockIdx.x;
+  constexpr int TPQ = MOTIF_THREADS / MOTIF_QB;
+  extern __shared__ double2 roots[];                                                    // den
+  double* vst = reinterpret_cast<double*>(roots + den);                                 // [pair][cell of chunk]
+  int* nst = reinterpret_cast<int*>(vst + MOTIF_PAIR_CHUNK * MOTIF_THREADS);             // [cell of chunk][3]
+  const int ql = threadIdx.x / TPQ, sub = threadIdx.x - ql * TPQ;
+  const int iq = blockIdx.x * MOTIF_QB + ql;
+  const bool qv = iq < nq;
   const int p0 = blockIdx.y * MOTIF_PAIR_CHUNK;
   const int np = min(MOTIF_PAIR_CHUNK, npairs - p0);
   for (int t = threadIdx.x; t < den; t += blockDim.x) {
@@ -122,47 +130,61 @@ motif_ft_roots_kernel(int nq, const int* __restrict__ mi, int den, int ncells, c
     sincospi(2.0 * (double)t / (double)den, &s, &c);
     roots[t] = make_double2(c, s);
   }
-  // m_d mod den in [0, den)
-  int m0 = mi[3 * iq] % den, m1 = mi[3 * iq + 1] % den, m2 = mi[3 * iq + 2] % den;
+  int m0 = qv ? mi[3 * iq] % den : 0, m1 = qv ? mi[3 * iq + 1] % den : 0, m2 = qv ? mi[3 * iq + 2] % den : 0;
   m0 += m0 < 0 ? den : 0;
   m1 += m1 < 0 ? den : 0;
   m2 += m2 < 0 ? den : 0;
-  __syncthreads();
   double accr[MOTIF_PAIR_CHUNK], acci[MOTIF_PAIR_CHUNK];
 #pragma unroll
   for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) { accr[j] = 0.0; acci[j] = 0.0; }
-  for (int n = threadIdx.x; n < ncells; n += blockDim.x) {
-    const int e = (m0 * ni[3 * n] + m1 * ni[3 * n + 1] + m2 * ni[3 * n + 2]) % den;
-    const double2 ph = roots[e];
+  for (int c0 = 0; c0 < ncells; c0 += MOTIF_THREADS) {
+    const int nc = min(MOTIF_THREADS, ncells - c0);
+    __syncthreads();   // the previous chunk is consumed (and the table is written)
+    if (threadIdx.x < nc) {
+      for (int j = 0; j < np; j++) vst[j * MOTIF_THREADS + threadIdx.x] = vtab[(int64_t)(p0 + j) * ncells + c0 + threadIdx.x];
+      nst[3 * threadIdx.x] = ni[3 * (c0 + threadIdx.x)];
+      nst[3 * threadIdx.x + 1] = ni[3 * (c0 + threadIdx.x) + 1];
+      nst[3 * threadIdx.x + 2] = ni[3 * (c0 + threadIdx.x) + 2];
+    }
+    __syncthreads();
+    for (int t = sub; t < nc; t += TPQ) {
+      const int e = (m0 * nst[3 * t] + m1 * nst[3 * t + 1] + m2 * nst[3 * t + 2]) % den;
+      const double2 ph = roots[e];
 #pragma unroll
-    for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
-      if (j < np) {
-        const double v = vtab[(int64_t)(p0 + j) * ncells + n];
-        accr[j] = fma(v, ph.x, accr[j]);
-        acci[j] = fma(v, ph.y, acci[j]);
+      for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
+        if (j < np) {
+          const double v = vst[j * MOTIF_THREADS + t];
+          accr[j] = fma(v, ph.x, accr[j]);
+          acci[j] = fma(v, ph.y, acci[j]);
+        }
       }
     }
   }
-  __shared__ double red[2][MOTIF_PAIR_CHUNK][MOTIF_THREADS / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // sum over the TPQ threads of each point (a fixed shuffle tree inside the half warp)
 #pragma unroll
-  for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
-    const double r = warp_sum(accr[j]);
-    const double i = warp_sum(acci[j]);
-    if (lane == 0) { red[0][j][warp] = r; red[1][j][warp] = i; }
-  }
-  __syncthreads();
-  if (threadIdx.x < np) {
-    const int j = threadIdx.x;
-    double r = 0.0, i = 0.0;
-    for (int w = 0; w < MOTIF_THREADS / 32; w++) { r += red[0][j][w]; i += red[1][j][w]; }
-    r *= inv_total;
-    i *= inv_total;
-    const int2 ab = pairs[p0 + j];
+  for (int j = 0; j < MOTIF_PAIR_CHUNK; j++)
+#pragma unroll
+    for (int o = TPQ / 2; o > 0; o >>= 1) {
+      accr[j] += __shfl_xor_sync(0xffffffffu, accr[j], o);
+      acci[j] += __shfl_xor_sync(0xffffffffu, acci[j], o);
+    }
+  if (sub == 0 && qv) {
     cd* o = out + (int64_t)iq * na * na;
-    o[ab.x * na + ab.y] = mk(r, i);
-    o[ab.y * na + ab.x] = mk(r, -i);
+#pragma unroll
+    for (int j = 0; j < MOTIF_PAIR_CHUNK; j++) {
+      if (j < np) {
+        const int2 ab = pairs[p0 + j];
+        const double r = accr[j] * inv_total, i = acci[j] * inv_total;
+        o[ab.x * na + ab.y] = mk(r, i);
+        o[ab.y * na + ab.x] = mk(r, -i);
+      }
+    }
   }
+}
+
+extern "C" size_t motif_roots_smem(int den) {
+  return (size_t)den * sizeof(double2) + (size_t)MOTIF_PAIR_CHUNK * MOTIF_THREADS * sizeof(double) +
+         (size_t)3 * MOTIF_THREADS * sizeof(int);
 }
 
 // deriv = 0: W itself; deriv = 1: dW/dr0.
