@@ -65,6 +65,47 @@ static cudaError_t upload(DBuf& b, const T* src, size_t n, cudaStream_t s) {
   return cudaSuccess;
 }
 
+// Nearest integer, halves away from zero (std::round) for the grid coordinates of the set-up (|x| < 2^52), by
+// truncating conversions that compile inline: these loops run over every k point and cell of every call.
+static inline double round_coord(double x) {
+  return x >= 0 ? (double)(long long)(x + 0.5) : -(double)(long long)(0.5 - x);
+}
+
+// Host-to-device copies of one call through the context's pinned staging buffer: a pageable source makes the
+// driver stage it copy by copy; here each source is copied into the pinned buffer on the host and sent with an
+// asynchronous copy.  The caller synchronises the stream before the buffer is written again.
+struct Stager {
+  xatu_ctx* ctx;
+  size_t off = 0;
+  template <typename V>
+  static size_t size(const V& v) {
+    return (v.size() * sizeof(typename V::value_type) + 15) / 16 * 16;
+  }
+  cudaError_t begin(size_t bytes) {
+    if (ctx->h_stage_bytes < bytes) {
+      if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+      ctx->h_stage = nullptr;
+      ctx->h_stage_bytes = 0;
+      const cudaError_t e = cudaMallocHost(&ctx->h_stage, bytes);
+      if (e != cudaSuccess) return e;
+      ctx->h_stage_bytes = bytes;
+    }
+    off = 0;
+    return cudaSuccess;
+  }
+  template <typename T>
+  cudaError_t put(DBuf& b, const T* src, size_t n) {
+    const cudaError_t e = b.ensure(std::max<size_t>(n * sizeof(T), 16));
+    if (e != cudaSuccess || !n) return e;
+    const size_t bytes = n * sizeof(T);
+    if (off + bytes > ctx->h_stage_bytes) return cudaErrorInvalidValue;
+    unsigned char* dst = static_cast<unsigned char*>(ctx->h_stage) + off;
+    memcpy(dst, src, bytes);
+    off += (bytes + 15) / 16 * 16;
+    return cudaMemcpyAsync(b.p, dst, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  }
+};
+
 extern "C" {
 
 int xatu_abi_version(void) { return 1; }
@@ -111,6 +152,7 @@ xatu_status xatu_ctx_destroy(xatu_ctx* ctx) {
                   &ctx->d_pp_P, &ctx->d_pp_E, &ctx->d_mesh_int, &ctx->d_cells_int};
   for (DBuf* b : bufs) b->release();
   if (ctx->h_small) cudaFreeHost(ctx->h_small);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->blas) cublasDestroy(ctx->blas);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
   for (auto& e : ctx->ev)
@@ -304,7 +346,7 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
         for (int a = 0; a < nd; a++) r0v[a] = red[a];
       for (int a = 0; a < nd; a++) {
         const double d = red[a] - r0v[a];
-        const double u = std::round(d);
+        const double u = round_coord(d);
         if (std::fabs(d - u) > 1e-6) ctx->kgrid_ok = false;
         ctx->kgrid[3 * i + a] = (int)u;
         if (i == 0 || (int)u < lo[a]) lo[a] = (int)u;
@@ -336,7 +378,7 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
         double red = 0.0;
         for (int b = 0; b < nd; b++) red += ctx->inv_gram[a * nd + b] * ind[b];
         red *= n_eff;
-        const double u = std::round(red);
+        const double u = round_coord(red);
         if (std::fabs(red - u) > 1e-6) ctx->ft_roots = false;
         ctx->mesh_int[3 * i + a] = (int)u;
       }
@@ -348,7 +390,7 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
       for (int a = 0; a < nd; a++) {
         const double f = (ctx->recip[3 * a] * R[0] + ctx->recip[3 * a + 1] * R[1] + ctx->recip[3 * a + 2] * R[2]) /
                          (2.0 * XATU_PI);
-        const double u = std::round(f);
+        const double u = round_coord(f);
         if (std::fabs(f - u) > 1e-6) ctx->ft_roots = false;
         long long v = (long long)u % n_eff;
         if (v < 0) v += n_eff;
@@ -356,21 +398,27 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
       }
     }
   }
-  XATU_CK(upload(ctx->d_kpoints, ctx->kpoints.data(), ctx->kpoints.size(), ctx->stream));
-  XATU_CK(upload(ctx->d_mesh, ctx->mesh.data(), ctx->mesh.size(), ctx->stream));
-  XATU_CK(upload(ctx->d_cells, ctx->cells.data(), ctx->cells.size(), ctx->stream));
-  if (ctx->ft_roots) {
-    XATU_CK(upload(ctx->d_mesh_int, ctx->mesh_int.data(), ctx->mesh_int.size(), ctx->stream));
-    XATU_CK(upload(ctx->d_cells_int, ctx->cells_int.data(), ctx->cells_int.size(), ctx->stream));
-  }
-  XATU_CK(upload(ctx->d_G, ctx->G.data(), ctx->G.size(), ctx->stream));
-  XATU_CK(upload(ctx->d_kgrid, ctx->kgrid.data(), ctx->kgrid.size(), ctx->stream));
   {
     std::vector<int2> pairs;
     for (int a = 0; a < ctx->natoms; a++)
       for (int b = a; b < ctx->natoms; b++) pairs.push_back(make_int2(a, b));
-    XATU_CK(upload(ctx->d_pairs, pairs.data(), pairs.size(), ctx->stream));
-    XATU_CK(upload(ctx->d_Q, ctx->Q, 3, ctx->stream));
+    // every array of the call goes through the pinned staging buffer (one host copy each, then asynchronous
+    // transfers; the synchronisation below frees the buffer for the next call)
+    Stager st{ctx};
+    const size_t need = st.size(ctx->kpoints) + st.size(ctx->mesh) + st.size(ctx->cells) + st.size(ctx->mesh_int) +
+                        st.size(ctx->cells_int) + st.size(ctx->G) + st.size(ctx->kgrid) + st.size(pairs) + 3 * 16;
+    XATU_CK(st.begin(need));
+    XATU_CK(st.put(ctx->d_kpoints, ctx->kpoints.data(), ctx->kpoints.size()));
+    XATU_CK(st.put(ctx->d_mesh, ctx->mesh.data(), ctx->mesh.size()));
+    XATU_CK(st.put(ctx->d_cells, ctx->cells.data(), ctx->cells.size()));
+    if (ctx->ft_roots) {
+      XATU_CK(st.put(ctx->d_mesh_int, ctx->mesh_int.data(), ctx->mesh_int.size()));
+      XATU_CK(st.put(ctx->d_cells_int, ctx->cells_int.data(), ctx->cells_int.size()));
+    }
+    XATU_CK(st.put(ctx->d_G, ctx->G.data(), ctx->G.size()));
+    XATU_CK(st.put(ctx->d_kgrid, ctx->kgrid.data(), ctx->kgrid.size()));
+    XATU_CK(st.put(ctx->d_pairs, pairs.data(), pairs.size()));
+    XATU_CK(st.put(ctx->d_Q, ctx->Q, 3));
   }
   XATU_CK(cudaStreamSynchronize(ctx->stream));
   ctx->has_exciton = true;

@@ -105,6 +105,8 @@ struct xatu_ctx {
   DBuf dv_V, dv_W, dv_T, dv_Y, dv_U, dv_R, dv_X, dv_Yf, dv_G, dv_tmp, dv_diagH, dv_small, dv_norm, dv_Bop, dv_Blo, dv_Uhi, dv_Ulo;
   DBuf dv_part;                // per-tile partial sums of the Davidson reductions
   void* h_small = nullptr;     // pinned host staging for small read-backs (4 KB)
+  void* h_stage = nullptr;     // pinned host staging of the exciton set-up's uploads
+  size_t h_stage_bytes = 0;
 
   // ---------------- adjoint
   bool bands_from_model = false;   // bands came from xatu_bands_compute (not uploaded)

@@ -79,13 +79,32 @@ std::vector<double> combinations(int n, int ndim, bool centered) {
   return out;
 }
 
+// Digits of the combinations in the order combinations() lists them (dimension 0 fastest), kept as a counter
+// that the caller advances, so that no list is built and no division is done per combination.
+struct CombinationCounter {
+  int n, ndim, shift, dig[3] = {0, 0, 0};
+  CombinationCounter(int n_, int ndim_, int shift_) : n(n_), ndim(ndim_), shift(shift_) {}
+  void get(double* c) const {
+    for (int d = 0; d < ndim; d++) c[d] = (double)dig[d] - shift;
+  }
+  void next() {
+    for (int d = 0; d < ndim; d++) {
+      if (++dig[d] < n) return;
+      dig[d] = 0;
+    }
+  }
+};
+
 std::vector<double> mp_mesh(int ndim, const double* recip, int n) {
-  std::vector<double> comb = combinations(n, ndim, false);
-  const long nk = (long)(comb.size() / ndim);
+  long nk = 1;
+  for (int d = 0; d < ndim; d++) nk *= n;
   std::vector<double> k((size_t)nk * 3, 0.0);
-  for (long i = 0; i < nk; i++) {
+  CombinationCounter cnt(n, ndim, 0);
+  for (long i = 0; i < nk; i++, cnt.next()) {
+    double cc[3];
+    cnt.get(cc);
     for (int j = 0; j < ndim; j++) {
-      double c = comb[(size_t)i * ndim + j];
+      double c = cc[j];
       if (n % 2 == 1) c += 1. / 2;
       const double f = (2 * c - n) / (2 * n);
       for (int x = 0; x < 3; x++) k[(size_t)i * 3 + x] += f * recip[3 * j + x];
@@ -95,12 +114,15 @@ std::vector<double> mp_mesh(int ndim, const double* recip, int n) {
 }
 
 std::vector<double> reduced_mesh(int ndim, const double* recip, int n, int factor) {
-  std::vector<double> comb = combinations(n, ndim, false);
-  const long nk = (long)(comb.size() / ndim);
+  long nk = 1;
+  for (int d = 0; d < ndim; d++) nk *= n;
   std::vector<double> k((size_t)nk * 3, 0.0);
-  for (long i = 0; i < nk; i++) {
+  CombinationCounter cnt(n, ndim, 0);
+  for (long i = 0; i < nk; i++, cnt.next()) {
+    double cc[3];
+    cnt.get(cc);
     for (int j = 0; j < ndim; j++) {
-      double c = comb[(size_t)i * ndim + j];
+      double c = cc[j];
       if (n % 2 == 1) c += 1. / 2;
       const double f = (2 * c - n) / (2 * n * factor);
       for (int x = 0; x < 3; x++) k[(size_t)i * 3 + x] += f * recip[3 * j + x];
@@ -110,14 +132,22 @@ std::vector<double> reduced_mesh(int ndim, const double* recip, int n, int facto
 }
 
 std::vector<double> truncate_supercell(int ndim, const double* basis, int ncell, double radius) {
-  std::vector<double> comb = combinations(ncell, ndim, true);
-  const long nc = (long)(comb.size() / ndim);
+  long nc = 1;
+  for (int d = 0; d < ndim; d++) nc *= ncell;
   std::vector<double> cells;
-  for (long i = 0; i < nc; i++) {
+  cells.reserve((size_t)nc * 3);
+  CombinationCounter cnt(ncell, ndim, ncell / 2);
+  for (long i = 0; i < nc; i++, cnt.next()) {
+    double cc[3];
+    cnt.get(cc);
     double v[3] = {0, 0, 0};
     for (int j = 0; j < ndim; j++)
-      for (int x = 0; x < 3; x++) v[x] += comb[(size_t)i * ndim + j] * basis[3 * j + x];
-    if (norm3(v) < radius + 1E-5) cells.insert(cells.end(), v, v + 3);
+      for (int x = 0; x < 3; x++) v[x] += cc[j] * basis[3 * j + x];
+    if (norm3(v) < radius + 1E-5) {
+      cells.push_back(v[0]);
+      cells.push_back(v[1]);
+      cells.push_back(v[2]);
+    }
   }
   return cells;
 }
