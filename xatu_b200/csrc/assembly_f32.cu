@@ -9,6 +9,7 @@
 #include <cstdlib>
 
 #include "assembly_panel.cuh"
+#include "engine.h"
 
 template <typename T, int NV, int NC, int NA, bool MIXED, int TK>
 __global__ void __launch_bounds__(TK * TK)
@@ -85,13 +86,13 @@ static cudaError_t launch_panel(const AsmParams& p, const AsmInputs& in, const A
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int grid = g.total < panel_num_sms() ? g.total : panel_num_sms();
-    kern<<<grid, XATU_PANEL_THREADS, g.smem, s>>>(p, in, out, g);
-    e = cudaGetLastError();
+    // the panel kernel and the mirror are launched chained (each waits for its predecessor grid at entry)
+    e = xatu_launch_chained(kern, dim3(grid), dim3(XATU_PANEL_THREADS), g.smem, s, p, in, out, g);
     if (e != cudaSuccess) return e;
     const unsigned nd = (unsigned)((p.N + XATU_KBLOCK - 1) / XATU_KBLOCK);
-    asm_diag_mirror_kernel<<<dim3(nd, 10), dim3(32, 8), 0, s>>>(reinterpret_cast<unsigned*>(out.Khi),
-                                                               reinterpret_cast<unsigned*>(out.Klo), p.N, p.ldk);
-    return cudaGetLastError();
+    return xatu_launch_chained(asm_diag_mirror_kernel, dim3(nd, 10), dim3(32, 8), 0, s,
+                               reinterpret_cast<unsigned*>(out.Khi), reinterpret_cast<unsigned*>(out.Klo), p.N,
+                               p.ldk);
   }
 }
 

@@ -886,6 +886,9 @@ bse_assemble_panel_kernel(AsmParams p, AsmInputs in, AsmOutputs out, AsmPanelGeo
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
   volatile int* abort = &s_abort;
+  // launched chained to the operand formatting: the set-up above overlaps its tail; no global memory is read
+  // before this point
+  xatu_grid_chain();
 
   if (warp >= XATU_PANEL_NCW) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(XATU_PANEL_REGS_PRODUCER));
@@ -913,6 +916,7 @@ bse_assemble_panel_kernel(AsmParams p, AsmInputs in, AsmOutputs out, AsmPanelGeo
 __global__ void asm_diag_mirror_kernel(unsigned* __restrict__ Kh, unsigned* __restrict__ Kl, long long N,
                                        long long ldk) {
   __shared__ unsigned th[32][33], tlo[32][33];
+  xatu_grid_chain();
   int q = blockIdx.y, si = 0;
   while (q > si) {
     q -= si + 1;

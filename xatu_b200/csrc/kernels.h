@@ -11,7 +11,7 @@ extern "C" __global__ void motif_ft_roots_kernel(int nq, const int* mi, int den,
                                                  int npairs, const int2* pairs, const double* vtab, double inv_total,
                                                  int na, cd* out);
 #define XATU_FT_MAXDEN 1536   // largest mesh denominator of the root-of-unity table (24 KB of shared memory)
-#define XATU_MOTIF_QB 16      // mesh points per CTA of motif_ft_roots_kernel
+#define XATU_MOTIF_QB 8       // mesh points per CTA of motif_ft_roots_kernel (a warp per point)
 extern "C" size_t motif_roots_smem(int den);
 extern "C" __global__ void recip_table_kernel(PotParams p, RecipTable t, int deriv, int nentries, const double* G,
                                               int na, const double* motif, cd* W);

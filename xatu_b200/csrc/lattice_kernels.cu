@@ -108,7 +108,7 @@ motif_ft_kernel(int nq, const double* __restrict__ q, int ncells, const double* 
 // motif_ft_kernel for a mesh and cells that are commensurate: q = sum_d (m_d / den) b_d and R = sum_d n_d a_d
 // with integers m, n, so that e^{i q.R} = e^{2 pi i (m.n mod den) / den} comes from a table of the den roots of
 // unity (sincospi of exact fractions) instead of one sincos per (q, cell).  One CTA per MOTIF_QB mesh points
-// (16 threads each) and chunk of pairs: the potentials of a chunk of cells are staged in shared memory once and
+// (MOTIF_THREADS / MOTIF_QB threads each) and chunk of pairs: the potentials of a chunk of cells are staged in shared memory once and
 // used by all of the CTA's points.  mi: nq x 3, ni: ncells x 3, every n_d reduced to [0, den).
 // Dynamic shared memory: motif_roots_smem(den).
 #define MOTIF_QB XATU_MOTIF_QB
