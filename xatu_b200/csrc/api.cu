@@ -71,6 +71,59 @@ static inline double round_coord(double x) {
   return x >= 0 ? (double)(long long)(x + 0.5) : -(double)(long long)(0.5 - x);
 }
 
+// Integer coordinates of points p (n x 3) in units of b_d / n_eff: red = n_eff inv(B B^T) B p, rounded; relative
+// to the first point when relative.  out: n x 3 (unused dimensions 0), lo / hi: the range per dimension.
+// Returns whether every point lies within 1e-6 of the grid.  Local copies of the small matrices keep the loop
+// free of reloads through the context.
+static bool grid_coords(const double* p, long n, int nd, const double* recip_in, const double* inv_in, int n_eff,
+                        bool relative, int* out, int* lo, int* hi) {
+  double rc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 3 * nd; i++) rc[i] = recip_in[i];
+  for (int i = 0; i < nd * nd; i++) iv[i] = inv_in[i];
+  double r0v[3] = {0, 0, 0};
+  bool ok = true;
+  for (int a = 0; a < 3; a++) lo[a] = hi[a] = 0;
+  for (long i = 0; i < n && ok; i++) {
+    const double* k = p + 3 * i;
+    double ind[3] = {0, 0, 0}, red[3] = {0, 0, 0};
+    for (int a = 0; a < nd; a++) ind[a] = rc[3 * a] * k[0] + rc[3 * a + 1] * k[1] + rc[3 * a + 2] * k[2];
+    for (int a = 0; a < nd; a++) {
+      for (int b = 0; b < nd; b++) red[a] += iv[a * nd + b] * ind[b];
+      red[a] *= n_eff;
+    }
+    if (i == 0 && relative)
+      for (int a = 0; a < nd; a++) r0v[a] = red[a];
+    for (int a = 0; a < nd; a++) {
+      const double d = red[a] - r0v[a];
+      const double u = round_coord(d);
+      if (std::fabs(d - u) > 1e-6) ok = false;
+      const int v = (int)u;
+      out[3 * i + a] = v;
+      if (i == 0 || v < lo[a]) lo[a] = v;
+      if (i == 0 || v > hi[a]) hi[a] = v;
+    }
+  }
+  return ok;
+}
+
+// Lattice coordinates n_d = b_d.R / 2 pi of cells R (n x 3), reduced to [0, n_eff); whether all are integers.
+static bool cell_coords(const double* R, long n, int nd, const double* recip_in, int n_eff, int* out) {
+  double rc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 3 * nd; i++) rc[i] = recip_in[i];
+  for (long i = 0; i < n; i++) {
+    const double* r = R + 3 * i;
+    for (int a = 0; a < nd; a++) {
+      const double f = (rc[3 * a] * r[0] + rc[3 * a + 1] * r[1] + rc[3 * a + 2] * r[2]) / (2.0 * XATU_PI);
+      const double u = round_coord(f);
+      if (std::fabs(f - u) > 1e-6) return false;
+      long long v = (long long)u % n_eff;
+      if (v < 0) v += n_eff;
+      out[3 * i + a] = (int)v;
+    }
+  }
+  return true;
+}
+
 // Host-to-device copies of one call through the context's pinned staging buffer: a pageable source makes the
 // driver stage it copy by copy; here each source is copied into the pinned buffer on the host and sent with an
 // asynchronous copy.  The caller synchronises the stream before the buffer is written again.
@@ -328,36 +381,15 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
     ctx->G.clear();
   // integer grid offsets of the k points in units of b_d / n_eff (reciprocal-mode table)
   ctx->kgrid.assign(3 * (size_t)e->nk, 0);
-  ctx->kgrid_ok = true;
   {
-    std::vector<double> r0v(3, 0.0);
-    const int nd = ctx->ndim;
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    for (int i = 0; i < e->nk && ctx->kgrid_ok; i++) {
-      const double* k = e->kpoints + 3 * i;
-      double ind[3] = {0, 0, 0}, red[3] = {0, 0, 0};
-      for (int a = 0; a < nd; a++)
-        ind[a] = ctx->recip[3 * a] * k[0] + ctx->recip[3 * a + 1] * k[1] + ctx->recip[3 * a + 2] * k[2];
-      for (int a = 0; a < nd; a++) {
-        for (int b = 0; b < nd; b++) red[a] += ctx->inv_gram[a * nd + b] * ind[b];
-        red[a] *= n_eff;
-      }
-      if (i == 0)
-        for (int a = 0; a < nd; a++) r0v[a] = red[a];
-      for (int a = 0; a < nd; a++) {
-        const double d = red[a] - r0v[a];
-        const double u = round_coord(d);
-        if (std::fabs(d - u) > 1e-6) ctx->kgrid_ok = false;
-        ctx->kgrid[3 * i + a] = (int)u;
-        if (i == 0 || (int)u < lo[a]) lo[a] = (int)u;
-        if (i == 0 || (int)u > hi[a]) hi[a] = (int)u;
-      }
-    }
+    ctx->kgrid_ok = grid_coords(e->kpoints, e->nk, ctx->ndim, ctx->recip.data(), ctx->inv_gram.data(), n_eff, true,
+                                ctx->kgrid.data(), lo, hi);
     ctx->rt_entries = 1;
     for (int a = 0; a < 3; a++) {
-      ctx->rt_span[a] = (a < nd) ? (hi[a] - lo[a]) : 0;
+      ctx->rt_span[a] = (a < ctx->ndim) ? (hi[a] - lo[a]) : 0;
       ctx->rt_len[a] = 2 * ctx->rt_span[a] + 1;
-      if (a < nd) ctx->rt_entries *= ctx->rt_len[a];
+      if (a < ctx->ndim) ctx->rt_entries *= ctx->rt_len[a];
     }
   }
   if (ctx->mode == XATU_MODE_RECIPROCAL && !ctx->kgrid_ok)
@@ -367,36 +399,16 @@ xatu_status xatu_exciton_set(xatu_ctx* ctx, const xatu_exciton_desc* e) {
   // n_d = b_d.R / 2 pi), for the root-of-unity phases of the motif FT
   ctx->ft_roots = ctx->mode == XATU_MODE_REALSPACE && n_eff <= XATU_FT_MAXDEN;
   if (ctx->ft_roots) {
-    const int nd = ctx->ndim;
+    int lo[3], hi[3];
     ctx->mesh_int.assign(3 * (size_t)nmesh, 0);
-    for (long long i = 0; i < nmesh && ctx->ft_roots; i++) {
-      const double* q = ctx->mesh.data() + 3 * i;
-      double ind[3] = {0, 0, 0};
-      for (int a = 0; a < nd; a++)
-        ind[a] = ctx->recip[3 * a] * q[0] + ctx->recip[3 * a + 1] * q[1] + ctx->recip[3 * a + 2] * q[2];
-      for (int a = 0; a < nd; a++) {
-        double red = 0.0;
-        for (int b = 0; b < nd; b++) red += ctx->inv_gram[a * nd + b] * ind[b];
-        red *= n_eff;
-        const double u = round_coord(red);
-        if (std::fabs(red - u) > 1e-6) ctx->ft_roots = false;
-        ctx->mesh_int[3 * i + a] = (int)u;
-      }
-    }
+    ctx->ft_roots = grid_coords(ctx->mesh.data(), nmesh, ctx->ndim, ctx->recip.data(), ctx->inv_gram.data(), n_eff,
+                                false, ctx->mesh_int.data(), lo, hi);
+  }
+  if (ctx->ft_roots) {
     const size_t ncl = ctx->cells.size() / 3;
     ctx->cells_int.assign(3 * ncl, 0);
-    for (size_t i = 0; i < ncl && ctx->ft_roots; i++) {
-      const double* R = ctx->cells.data() + 3 * i;
-      for (int a = 0; a < nd; a++) {
-        const double f = (ctx->recip[3 * a] * R[0] + ctx->recip[3 * a + 1] * R[1] + ctx->recip[3 * a + 2] * R[2]) /
-                         (2.0 * XATU_PI);
-        const double u = round_coord(f);
-        if (std::fabs(f - u) > 1e-6) ctx->ft_roots = false;
-        long long v = (long long)u % n_eff;
-        if (v < 0) v += n_eff;
-        ctx->cells_int[3 * i + a] = (int)v;
-      }
-    }
+    ctx->ft_roots = cell_coords(ctx->cells.data(), (long)ncl, ctx->ndim, ctx->recip.data(), n_eff,
+                                ctx->cells_int.data());
   }
   {
     std::vector<int2> pairs;
