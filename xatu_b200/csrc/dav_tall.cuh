@@ -172,6 +172,82 @@ __host__ __device__ inline size_t ts_update_smem(int a, int b, int TR) {
   return ((size_t)2 * TR * (b + 1) + (size_t)TR * (a + 1) + (size_t)a * b + (size_t)b * b) * sizeof(cd);
 }
 
+// ts_update_kernel fused with the projection that follows it in the orthonormalisation: Out = (In - A C) S per row
+// tile as above, then the tile's partial of [A[:, 0:pa], Out]^H Out from the rows still in shared memory
+// (pa = a or 0): part[tile][r + c (pa + b)], r < pa + b, c < b (added in tile order by ts_sum_kernel).
+// Shared memory: ts_update_smem(a, b, TR).
+__global__ void __launch_bounds__(TS_THREADS)
+ts_update_proj_kernel(const cd* In, int b, const cd* __restrict__ A, int a, const cd* __restrict__ C, int ldc,
+                      const cd* __restrict__ S, cd* Out, long long N, int TR, int pa, cd* __restrict__ part) {
+  xatu_grid_chain();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cd* sI = reinterpret_cast<cd*>(smem_raw);   // TR x (b + 1)
+  cd* sO = sI + TR * (b + 1);                 // TR x (b + 1): In - A C
+  cd* sA = sO + TR * (b + 1);                 // TR x (a + 1)
+  cd* sC = sA + TR * (a + 1);                 // a x b row-major
+  cd* sS = sC + a * b;                        // b x b row-major
+  const long long row0 = (long long)blockIdx.x * TR;
+  ts_stage(sI, b + 1, In, b, N, row0, TR);
+  if (a > 0) ts_stage(sA, a + 1, A, a, N, row0, TR);
+  for (int t = threadIdx.x; t < a * b; t += TS_THREADS) {
+    const int r = t / b, c = t - r * b;
+    sC[t] = C[r + (size_t)c * ldc];
+  }
+  if (S)
+    for (int t = threadIdx.x; t < b * b; t += TS_THREADS) {
+      const int r = t / b, c = t - r * b;
+      sS[t] = S[r + (size_t)c * b];
+    }
+  ts_cp_wait();
+  __syncthreads();
+  const cd* src = sI;
+  if (a > 0) {
+    for (int t = threadIdx.x; t < TR * b; t += TS_THREADS) {
+      const int x = t % TR, c = t / TR;
+      cd s = sI[x * (b + 1) + c];
+#pragma unroll 4
+      for (int r = 0; r < a; r++) s = s - sA[x * (a + 1) + r] * sC[r * b + c];
+      sO[x * (b + 1) + c] = s;
+    }
+    __syncthreads();
+    src = sO;
+  }
+  cd* sF = a > 0 ? sI : sO;   // the tile of Out (rows past N are zero, as the staged rows are)
+  for (int t = threadIdx.x; t < TR * b; t += TS_THREADS) {
+    const int x = t % TR, c = t / TR;
+    const long long i = row0 + x;
+    cd v;
+    if (S) {
+      v = mk(0, 0);
+#pragma unroll 4
+      for (int r = 0; r < b; r++) v = v + src[x * (b + 1) + r] * sS[r * b + c];
+    } else {
+      v = src[x * (b + 1) + c];
+    }
+    sF[x * (b + 1) + c] = v;
+    if (i < N) Out[(long long)c * N + i] = v;
+  }
+  __syncthreads();
+  const int na = pa + b, ab = na * b;
+  cd* mine = part + (size_t)blockIdx.x * ab;
+  for (int o = threadIdx.x; o < ab; o += TS_THREADS) {
+    const int r = o % na, c = o / na;
+    const cd* u = r < pa ? sA + r : sF + (r - pa);
+    const int us = r < pa ? a + 1 : b + 1;
+    double sx0 = 0.0, sy0 = 0.0, sx1 = 0.0, sy1 = 0.0;
+#pragma unroll 4
+    for (int x = 0; x < TR; x += 2) {
+      const cd u0 = u[x * us], v0 = sF[x * (b + 1) + c];
+      const cd u1 = u[(x + 1) * us], v1 = sF[(x + 1) * (b + 1) + c];
+      sx0 = fma(u0.x, v0.x, fma(u0.y, v0.y, sx0));
+      sy0 = fma(u0.x, v0.y, fma(-u0.y, v0.x, sy0));
+      sx1 = fma(u1.x, v1.x, fma(u1.y, v1.y, sx1));
+      sy1 = fma(u1.x, v1.y, fma(-u1.y, v1.x, sy1));
+    }
+    mine[o] = mk(sx0 + sx1, sy0 + sy1);
+  }
+}
+
 // Ritz vectors and preconditioned residuals of the lowest k Ritz pairs, per row tile (TR a multiple of 32):
 //   U = V Y, WU = W Y (V, W: N x m; Y: m x k, leading dimension ldy),
 //   r_c = WU_c - theta_c U_c,  P_c = r_c / (theta_c - H_ii)  (|denominator| >= 1e-8),

@@ -390,6 +390,20 @@ static xatu_status ts_update(xatu_ctx* ctx, const cd* In, int b, const cd* A, in
   return XATU_OK;
 }
 
+// Out = (In - A C) S (ts_update), then Z[0 : pa + b, 0 : b] = [A[:, 0:pa], Out]^H Out from the same row tiles.
+static xatu_status ts_update_proj(xatu_ctx* ctx, const cd* In, int b, const cd* A, int a, const cd* C, int ldc,
+                                  const cd* S, cd* Out, long long N, int pa, cd* Z, int ldz) {
+  const int TR = ts_pick_tile([&](int tr) { return ts_update_smem(a, b, tr); }, 16);
+  const int G = (int)((N + TR - 1) / TR);
+  const int ab = (pa + b) * b;
+  XATU_TRY(ts_part_ensure(ctx, (size_t)G * ab * sizeof(cd)));
+  XATU_CHAIN(ts_update_proj_kernel, G, TS_THREADS, ts_update_smem(a, b, TR), In, b, A, a, C, ldc, S, Out, N, TR, pa,
+             ctx->dv_part.as<cd>());
+  XATU_CHAIN(ts_sum_kernel, (ab + 31) / 32, TS_SUM_THREADS, 0, ctx->dv_part.as<cd>(), G, ab, pa + b, Z, ldz,
+             ctx->d_status.as<int>(), static_cast<double*>(nullptr));
+  return XATU_OK;
+}
+
 // Orthonormalise the block t = V[:, m : m + nsel] against V[:, 0 : m] and within itself:
 //   t <- t - V (V^H t);
 //   Z = [V t]^H t: C = V^H t, G = t^H t - C^H C; Cholesky of G with dropping -> S;  X = (t - V C) S;
@@ -405,13 +419,15 @@ static xatu_status orthonormalize_block(xatu_ctx* ctx, long long N, int m, int n
   cd* S = Z + (size_t)DAV_MAX_BASIS * DAV_MAX_BASIS / 2;   // nsel x nsel (nsel <= DAV_MAX_BASIS / 2)
   int* dkept = reinterpret_cast<int*>(ctx->dv_norm.as<double>() + 1024);
   if (m > 0) {
+    // t <- t - V (V^H t), and Z = [V t]^H t from the updated row tiles
     XATU_TRY(ts_proj(ctx, V, m, t, nsel, N, Z, ldZ));
-    XATU_TRY(ts_update(ctx, t, nsel, V, m, Z, ldZ, nullptr, t, N));
+    XATU_TRY(ts_update_proj(ctx, t, nsel, V, m, Z, ldZ, nullptr, t, N, m, Z, ldZ));
+  } else {
+    XATU_TRY(ts_proj(ctx, t, nsel, t, nsel, N, Z, ldZ));
   }
-  XATU_TRY(ts_proj(ctx, V, m + nsel, t, nsel, N, Z, ldZ));
   XATU_CHAIN(ts_gram_orth_kernel, 1, 32, ts_gram_orth_smem(m, nsel), Z, ldZ, m, nsel, 1e-20, S, dkept);
-  XATU_TRY(ts_update(ctx, t, nsel, m > 0 ? V : nullptr, m, Z, ldZ, S, X, N));
-  XATU_TRY(ts_proj(ctx, X, nsel, X, nsel, N, Z, ldZ));
+  // X = (t - V Z[0:m]) S, and Z = X^H X from the same row tiles
+  XATU_TRY(ts_update_proj(ctx, t, nsel, m > 0 ? V : nullptr, m, Z, ldZ, S, X, N, 0, Z, ldZ));
   XATU_CHAIN(ts_gram_orth_kernel, 1, 32, ts_gram_orth_smem(0, nsel), Z, ldZ, 0, nsel, 1e-24, S, dkept);
   XATU_TRY(ts_update(ctx, X, nsel, nullptr, 0, nullptr, 0, S, t, N));
   return XATU_OK;
@@ -498,6 +514,7 @@ xatu_status xatu_davidson_solve(xatu_ctx* ctx, int nstates, double* eigval, doub
     const int bmax = DAV_MAX_BASIS / 2;
     XATU_CK(xatu_raise_smem_limit((const void*)ts_proj_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_update_kernel, 224 * 1024));
+    XATU_CK(xatu_raise_smem_limit((const void*)ts_update_proj_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_ritz_kernel, 224 * 1024));
     XATU_CK(xatu_raise_smem_limit((const void*)ts_gram_orth_kernel, ts_gram_orth_smem(DAV_MAX_BASIS - bmax, bmax)));
   }
