@@ -337,13 +337,25 @@ ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop
   cd* A = reinterpret_cast<cd*>(smem_raw);        // b x b row-major, lower triangle -> L
   cd* M = A + b * b;                              // L_k^{-1}, row-major
   cd* Zs = M + b * b;                             // Z[0 : m + b, 0 : b], column-major (ld m + b)
-  int* idx = reinterpret_cast<int*>(Zs + (size_t)(m + b) * b);   // kept column indices
+  double* rdg = reinterpret_cast<double*>(Zs + (size_t)(m + b) * b);   // 1 / L_ii of the kept columns
+  int* idx = reinterpret_cast<int*>(rdg + b);                            // kept column indices
   const int lane = threadIdx.x;
   const int mz = m + b;
-  // stage the block of Z (coalesced along each column), then G = Z[m:, :] - Z[:m, :]^H Z[:m, :] from shared memory
-  for (int t = lane; t < mz * b; t += 32) {
-    const int q = t % mz, c = t / mz;
-    Zs[t] = Z[q + (size_t)c * ldz];
+  // stage the block of Z (coalesced along each column), eight loads per lane in flight before their stores so
+  // that the warp waits for L2 once per batch, then G = Z[m:, :] - Z[:m, :]^H Z[:m, :] from shared memory
+  const int tot = mz * b;
+  for (int t0 = 0; t0 < tot; t0 += 8 * 32) {
+    cd v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int t = t0 + u * 32 + lane;
+      if (t < tot) v[u] = Z[t % mz + (size_t)(t / mz) * ldz];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int t = t0 + u * 32 + lane;
+      if (t < tot) Zs[t] = v[u];
+    }
   }
   __syncwarp();
   for (int t = lane; t < b * b; t += 32) {
@@ -381,14 +393,17 @@ ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop
     }
     __syncwarp();
   }
-  // M = L_k^{-1} (lower triangular, nk x nk): lane j solves column j by forward substitution
+  // M = L_k^{-1} (lower triangular, nk x nk): lane j solves column j by forward substitution, with the
+  // reciprocal pivots formed once per kept column instead of once per (row, column) pair
+  for (int i = lane; i < nk; i += 32) rdg[i] = 1.0 / A[idx[i] * b + idx[i]].x;
+  __syncwarp();
   for (int j = lane; j < nk; j += 32) {
     for (int i = 0; i < nk; i++) M[i * b + j] = mk(0, 0);
-    M[j * b + j] = mk(1.0 / A[idx[j] * b + idx[j]].x, 0.0);
+    M[j * b + j] = mk(rdg[j], 0.0);
     for (int i = j + 1; i < nk; i++) {
       cd sum = mk(0, 0);
       for (int l = j; l < i; l++) sum = sum + A[idx[i] * b + idx[l]] * M[l * b + j];
-      const double rd = 1.0 / A[idx[i] * b + idx[i]].x;
+      const double rd = rdg[i];
       M[i * b + j] = mk(-sum.x * rd, -sum.y * rd);
     }
   }
@@ -407,5 +422,5 @@ ts_gram_orth_kernel(const cd* __restrict__ Z, int ldz, int m, int b, double drop
 }
 
 __host__ __device__ inline size_t ts_gram_orth_smem(int m, int b) {
-  return (size_t)(2 * b * b + (m + b) * b) * sizeof(cd) + (size_t)b * sizeof(int);
+  return (size_t)(2 * b * b + (m + b) * b) * sizeof(cd) + (size_t)b * (sizeof(double) + sizeof(int));
 }
